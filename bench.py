@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Full-graph dependency-tree build on RMAT-22: GTEPS through the C ABI.
+
+Workload (one step): build_tree from scratch (core/graph.hpp:873-985) of
+SSSP (default; --algo bfs|sssp|sswp|wcc) over a directed RMAT graph of scale 22
+(4,194,304 vertices, 67,108,864 edges, a/b/c = .57/.19/.19, duplicates and
+self-loops kept, seeded order), weights splitmix64(src<<32|dst) % 255 + 1,
+rooted at the highest out-degree vertex.  The graph is resident in HBM; the
+edge pool (>0.5 GB) is larger than L2, so no flush is needed between steps.
+
+value  = reached edges / device time per build (GTEPS), CUDA events on the
+         stream the library launches on, max over ranks.
+e2e    = the same through the public API with the result read back: every
+         step calls rg_build_tree and copies the value array into pinned host
+         memory; wall clock.
+--impl reference runs the reference's own CPU build_tree (oracle/_ref, the
+reference's core/graph.hpp compiled with an OpenMP stand-in for TBB) on the
+host cores.  Multi-GPU: independent replicas, one per rank (the path does not
+shard); no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "updates/s at p99≤1ms (served vs per-update GPU); full-graph GTEPS vs HBM"
+WEIGHTED = {"bfs": False, "sssp": True, "sswp": True, "wcc": False}
+THROTTLE_BITS = {
+    0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+    0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+    0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--algo", default="sssp", choices=list(WEIGHTED))
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-timeout", type=float, default=240.0)
+    return ap.parse_args()
+
+
+def workload(args):
+    return {"workload": f"full-graph {args.algo.upper()} build_tree, RMAT-{args.scale} "
+                        f"(V=2^{args.scale}, E=16*V, a/b/c=.57/.19/.19, seed {args.seed}), "
+                        f"weights splitmix64(src<<32|dst)%255+1, root = max out-degree vertex",
+            "scale": args.scale, "algo": args.algo, "seed": args.seed,
+            "l2": "inputs larger than L2 (edge pool > 126 MB); no flush"}
+
+
+def make_graph_input(args):
+    from risgraph_b200 import gen
+    pairs = gen.rmat(args.scale, seed=args.seed)
+    V = 1 << args.scale
+    root = gen.max_out_degree_vertex(pairs, V)
+    return pairs, V, root
+
+
+def reached_edges(pairs, V, values, algo):
+    """Distinct stored edges out of reached vertices (both directions for WCC)."""
+    src = pairs[:, 0].astype(np.int64)
+    dst = pairs[:, 1].astype(np.int64)
+    if algo == "wcc":
+        key = np.unique(np.concatenate([src * V + dst, dst * V + src]))
+        return int(len(key)), V
+    init = {"bfs": 65536, "sssp": 134217728, "sswp": 0}[algo]
+    reached = values != init
+    key = np.unique(src * V + dst)
+    ks = key // V
+    return int(reached[ks].sum()), int(reached.sum())
+
+
+def algorithmic_bytes(V, V_r, E_r, algo):
+    s_e = 16 if WEIGHTED[algo] else 8
+    return 16 * V + 16 * V_r + E_r * (s_e + 8)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 3:
+                try:
+                    self.samples.append((float(parts[0]), float(parts[1]), int(parts[2], 16)))
+                except ValueError:
+                    pass
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(s[0] for s in self.samples)
+        mask = 0
+        for s in self.samples:
+            mask |= s[2]
+        reasons = [n for b, n in THROTTLE_BITS.items() if mask & b and n != "gpu_idle"]
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(s[1] for s in self.samples), "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def cpu_reference(pairs, V, root, algo, repeats, warmup, timeout):
+    """The reference's own build_tree (oracle/_ref) on all host cores."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None, "oracle/_ref/ref_driver not built"
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory(prefix="rg_bench_") as tmp:
+        path = os.path.join(tmp, "g.bin")
+        pairs.tofile(path)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="true")
+        cmd = [O.REF_DRIVER, "build", algo, path, str(V), str(root), os.path.join(tmp, "out"), str(repeats),
+               str(warmup)]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
+        except subprocess.TimeoutExpired:
+            return None, f"reference build timed out after {timeout}s"
+        if r.returncode != 0:
+            return None, f"reference driver failed: {r.stderr[-200:]}"
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        vals = np.fromfile(os.path.join(tmp, "out.val"), dtype=np.uint64)
+    info["threads"] = threads
+    return (info, vals), None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pairs, V, root = make_graph_input(args)
+    res, err = cpu_reference(pairs, V, root, args.algo, args.steps, args.warmup, 1800)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    info, vals = res
+    E_r, V_r = reached_edges(pairs, V, vals, args.algo)
+    t = float(np.mean(info["build_times"]))
+    value = E_r / t / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": workload(args),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": info["threads"], "kind": "reference",
+                             "sample": f"RMAT-{args.scale} {args.algo} build_tree x{args.steps} after "
+                                       f"{args.warmup} warm-up (load {info['load_s']:.1f}s untimed)"},
+            "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import risgraph_b200 as rg
+
+    pairs, V, root = make_graph_input(args)
+    algo = args.algo
+    directed = algo != "wcc"
+    g = rg.Graph(V, len(pairs), symmetric=not directed, weighted=WEIGHTED[algo])
+    g.add_pairs(pairs, directed, want_old=False)
+    stream = torch.cuda.Stream()
+    g.set_stream(stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        g.build_tree(algo, root)
+    values = g.values()
+    E_r, V_r = reached_edges(pairs, V, values, algo)
+
+    # timed region: device time with CUDA events on the launching stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    l0 = g.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for a, b in ev:
+            a.record(stream)
+            g.build_tree(algo, root)
+            b.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = g.launch_count() - l0
+    times = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(times))
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = E_r * args.steps * world / (total_ms / 1e3) / 1e9
+
+    # end to end through the API: build + value readback into pinned memory
+    host_vals = torch.empty(V, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    import ctypes
+    L = rg.lib()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.build_tree(algo, root)
+        rc = L.rg_get_labels(g._h, ctypes.c_void_p(host_vals.ctypes.data), None, None)
+        assert rc == 0
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    assert np.array_equal(host_vals, values)
+    e2e = E_r * args.steps * world / e2e_s / 1e9
+
+    # roofline of the level-relaxation kernels (k_push + k_push_hub)
+    g.profile(True)
+    g.profile_read()
+    nb = 3
+    for _ in range(nb):
+        g.build_tree(algo, root)
+    plaunch, pms = g.profile_read()
+    g.profile(False)
+    push_ms_per_build = pms / nb
+    alg = algorithmic_bytes(V, V_r, E_r, algo)
+    peak, peak_kind = load_peaks()
+    achieved = alg / (push_ms_per_build / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "traffic": None, "kernel": "k_push+k_push_hub (all levels of one build)",
+            "algorithmic_bytes": alg, "launches_per_build": plaunch / nb, "kernel_ms_per_build": push_ms_per_build}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res, err = cpu_reference(pairs, V, root, algo, 2, 1, args.cpu_timeout)
+        if res is None:
+            cpu = {"value": None, "unit": "GTEPS", "cores": os.cpu_count(), "kind": "reference", "sample": err}
+        else:
+            info, vals = res
+            ok = bool(np.array_equal(vals, values))
+            t = float(np.mean(info["build_times"]))
+            cpu = {"value": E_r / t / 1e9, "unit": "GTEPS", "cores": info["threads"], "kind": "reference",
+                   "sample": f"RMAT-{args.scale} {algo} build_tree x2 after 1 warm-up "
+                             f"(load {info['load_s']:.1f}s untimed)", "values_match_gpu": ok}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": workload(args), "clocks": clk.summary(),
+                "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": V * 8},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+                "reached": {"V_r": V_r, "E_r": E_r}}
+        print(json.dumps(line))
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

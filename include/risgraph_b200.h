@@ -1,0 +1,157 @@
+/* risgraph_b200: B200-native (sm_100a) incremental dependency-tree maintenance
+ * for BFS / SSSP / SSWP / WCC under edge insertions and deletions.
+ *
+ * Drop-in C ABI for the hot path of the reference's header-only
+ * template<EdgeData> class Graph (core/graph.hpp:41-1908).  The reference takes
+ * its per-algorithm semantics as lambda template parameters; a C ABI cannot, so
+ * an algorithm enum selects the four hook sets the reference's drivers define
+ * (src/bfs.cpp:76-91, src/sssp.cpp:67-91, src/sswp.cpp:76-91, src/wcc.cpp:62-86).
+ * The adjacency and the label array live in device memory (HBM); the host
+ * mirror is filled on rg_get_labels.  Plain pointers and sizes only; no
+ * exceptions cross the ABI: every call returns an rg_status.
+ *
+ * Threading: one CUDA stream per graph; calls on one graph are serialised by
+ * the caller (the reference's build_tree / update_tree_* are single-caller,
+ * core/graph.hpp:1728).  Distinct graphs may be used from distinct threads.
+ * Every call returns after its device work has completed.
+ *
+ * Limits of the device layout: vertices < 2^31 and, for weighted graphs,
+ * edge weights < 2^31 (the reference stores 48-bit ids and 64-bit weights);
+ * edge multiplicities are 32-bit (the reference's are 16-bit,
+ * core/type.hpp:24).  Out-of-range input returns an error, never a fault. */
+#ifndef RISGRAPH_B200_H
+#define RISGRAPH_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference throws std::runtime_error("VertexId error.")
+ * for ids >= |V| (core/graph.hpp:205,231); here that is RG_EINVAL_VID. */
+typedef enum {
+  RG_OK = 0,
+  RG_EINVAL = 1,        /* bad argument (null graph, bad algorithm, size) */
+  RG_EINVAL_VID = 2,    /* vertex id >= |V| */
+  RG_EINVAL_WEIGHT = 3, /* weight >= 2^31 on a weighted graph */
+  RG_ENOMEM_HBM = 4,    /* device allocation failed / HBM budget exceeded */
+  RG_ENOSPACE = 5,      /* edge pool or edge index full */
+  RG_ETIMEOUT = 6,      /* a bounded device wait gave up */
+  RG_ECUDA = 7,         /* CUDA runtime error (message in rg_last_error) */
+  RG_ESTATE = 8         /* call not valid in the graph's current state */
+} rg_status;
+
+/* Algorithms: the a8 hook sets of the reference drivers. */
+typedef enum { RG_BFS = 0, RG_SSSP = 1, RG_SSWP = 2, RG_WCC = 3 } rg_algo;
+
+/* Edge<EdgeData> (core/type.hpp:57-81): src, dst, data (weight; ignored on
+ * unweighted graphs). 24 bytes, host byte order. */
+typedef struct {
+  uint64_t src, dst, data;
+} rg_edge;
+
+typedef struct rg_graph rg_graph;
+
+/* Graph(vertices, hint_edges, symmetric, dual, trace_modified)
+ * (core/graph.hpp:61-100), plus `weighted` (Graph<uint64_t> vs Graph<void>).
+ * hint_edges sizes the device edge pool and index (0 = 16 * vertices, the
+ * reference's default at :64). */
+int rg_create(uint64_t vertices, uint64_t hint_edges, int symmetric, int dual, int trace_modified,
+              int weighted, rg_graph **out);
+int rg_destroy(rg_graph *g);
+
+/* Graph::add_edge / del_edge for n edges (core/graph.hpp:203-253), applied as
+ * one batch.  old_num[i] (nullable) receives the multiplicity before edge i,
+ * with the reference's undirected conventions (:206-211, :232-237). */
+int rg_add_edges(rg_graph *g, const rg_edge *edges, uint64_t n, int directed, uint64_t *old_num);
+int rg_del_edges(rg_graph *g, const rg_edge *edges, uint64_t n, int directed, uint64_t *old_num);
+
+/* The same for edges given in the reference's binary file format
+ * (mmap_binary, core/io.hpp:26-36): n (src,dst) uint64 pairs.  Weights are
+ * splitmix64(src<<32|dst) % 255 + 1 on weighted graphs (rg_gen_weight). */
+int rg_add_pairs(rg_graph *g, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num);
+int rg_del_pairs(rg_graph *g, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num);
+
+/* Graph::get_edge_num (core/graph.hpp:198-201) for n edges. */
+int rg_get_edge_num(rg_graph *g, const rg_edge *edges, uint64_t n, uint64_t *num);
+
+/* get_outgoing_degree / get_incoming_degree (core/graph.hpp:165-174) for all
+ * vertices: sum of multiplicities (IndexedEdgeStorage::get_degree,
+ * core/storage.hpp:329).  Either pointer may be NULL. */
+int rg_get_degrees(rg_graph *g, uint64_t *out_degree, uint64_t *in_degree);
+
+/* Graph::build_tree (core/graph.hpp:873-985) with the hooks of `algo` rooted
+ * at `root` (ignored for WCC).  Sets the graph's label algorithm and root for
+ * the update calls below.  total (nullable) = number of label updates. */
+int rg_build_tree(rg_graph *g, int algo, uint64_t root, uint64_t *total);
+
+/* Graph::update_tree_add for one edge (n == 1, core/graph.hpp:1124-1160) or a
+ * batch (core/graph.hpp:1162-1218).  The edges are already in the adjacency. */
+int rg_update_tree_add(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int directed, uint64_t *total);
+
+/* Graph::update_tree_del for one edge (core/graph.hpp:1622-1656) or a batch
+ * (core/graph.hpp:1658-1718).  The edges are already removed. */
+int rg_update_tree_del(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int directed, uint64_t *total);
+
+/* need_update_tree_add (core/graph.hpp:987-1000) and need_update_tree_del
+ * (core/graph.hpp:1220-1233) for n edges: unsafe[i] = 1 when edge i needs a
+ * tree repair.  is_del (nullable = all adds) selects the hook per edge. */
+int rg_classify(rg_graph *g, int algo, const rg_edge *edges, const uint8_t *is_del, uint64_t n, int directed,
+                uint8_t *unsafe);
+
+/* The batch driver step of src/sssp_inc_batch.cpp:141-157 (resp. :159-175)
+ * fused on the device: add (resp. delete) the n edges, then repair the tree for
+ * exactly those whose multiplicity went 0->1 (resp. 1->0).  No host decision
+ * in between.  old_num as for rg_add_edges. */
+int rg_apply_add(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int directed, uint64_t *old_num);
+int rg_apply_del(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int directed, uint64_t *old_num);
+
+/* rg_apply_add / rg_apply_del over reference-format pairs (see rg_add_pairs). */
+int rg_apply_add_pairs(rg_graph *g, int algo, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num);
+int rg_apply_del_pairs(rg_graph *g, int algo, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num);
+
+/* Labels (VertexTree, core/graph.hpp:54-59): value, parent vertex (== |V| for
+ * none, as empty_parent at :90) and parent edge weight.  Any pointer may be NULL. */
+int rg_get_labels(rg_graph *g, uint64_t *value, uint64_t *parent, uint64_t *parent_w);
+
+/* Vertices whose label changed since rg_clear_modified (trace_modified graphs;
+ * get_modified / clear_modified, core/graph.hpp:117-130).  Writes up to cap ids. */
+int rg_get_modified(rg_graph *g, uint64_t *vids, uint64_t cap, uint64_t *n);
+int rg_clear_modified(rg_graph *g);
+
+/* Checksum of the value array on the device (same definition as
+ * rg_gen_value_checksum), so per-step checks need no label copy. */
+int rg_value_checksum(rg_graph *g, uint64_t *checksum);
+
+/* Counters of the last tree call: levels run, vertices invalidated by deletion
+ * repair, full recomputes.  Any pointer may be NULL. */
+int rg_last_stats(rg_graph *g, uint64_t *levels, uint64_t *invalidated, uint64_t *recomputes);
+
+/* Run this graph's device work on a caller-provided cudaStream_t (NULL:
+ * back to the graph's own stream), e.g. to time it with events on that stream
+ * or to order it after the caller's copies.  rg_get_stream returns the stream
+ * in use.  No reference counterpart: the reference runs on host threads. */
+int rg_set_stream(rg_graph *g, void *cuda_stream);
+int rg_get_stream(rg_graph *g, void **cuda_stream);
+
+/* Kernel accounting.  rg_launch_count: kernels this graph has launched since
+ * creation.  rg_profile(g, 1) brackets every level-relaxation launch (the
+ * push kernels) with CUDA events on the launching stream; rg_profile_read
+ * returns their number and summed device time in milliseconds since the last
+ * read.  No reference counterpart (the reference prints phase wall times). */
+int rg_launch_count(rg_graph *g, uint64_t *launches);
+int rg_profile(rg_graph *g, int enable);
+int rg_profile_read(rg_graph *g, uint64_t *launches, double *ms);
+
+/* Device bytes held by the graph. */
+int rg_device_bytes(rg_graph *g, uint64_t *bytes);
+
+const char *rg_status_string(int status);
+/* Last error message of the calling thread ("" if none). */
+const char *rg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

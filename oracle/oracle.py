@@ -118,6 +118,12 @@ class OracleGraph:
     def get_edge_num(self, s, d, w=0):
         return lib().rgo_get_edge_num(self.h, s, d, w)
 
+    def out_degree(self, v):
+        return int(lib().rgo_get_outgoing_degree(self.h, v))
+
+    def in_degree(self, v):
+        return int(lib().rgo_get_incoming_degree(self.h, v))
+
     def build_tree(self, root=0):
         return lib().rgo_build_tree(self.h, self.a, root)
 

@@ -1,0 +1,334 @@
+"""risgraph_b200: B200-native incremental dependency-tree maintenance.
+
+Python view of the C ABI in include/risgraph_b200.h, shaped like the
+reference's Graph (core/graph.hpp:41): the same method names (add_edge,
+del_edge, build_tree, update_tree_add, update_tree_del, need_update_tree_add,
+need_update_tree_del), with the per-algorithm hooks chosen by name
+("bfs", "sssp", "sswp", "wcc") instead of lambdas.  All work runs in
+librisgraph_b200.so on the GPU; there is no CPU fallback, and a missing or
+unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+__all__ = ["Graph", "RGError", "EDGE_DTYPE", "ALGOS", "lib", "gen", "LIB_PATH"]
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "librisgraph_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "risgraph_b200.h")
+
+ALGOS = {"bfs": 0, "sssp": 1, "sswp": 2, "wcc": 3}
+EDGE_DTYPE = np.dtype([("src", "<u8"), ("dst", "<u8"), ("data", "<u8")])  # rg_edge
+
+_u64 = ctypes.c_uint64
+_ptr = ctypes.c_void_p
+_int = ctypes.c_int
+_lib = None
+
+
+class RGError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        L = lib()
+        msg = L.rg_last_error().decode() or L.rg_status_string(status).decode()
+        super().__init__(f"{where}: {msg} (status {status})")
+        self.status = status
+
+
+def _declare(L):
+    P = _ptr
+    sig = {
+        "rg_create": [_u64, _u64, _int, _int, _int, _int, P],
+        "rg_destroy": [P],
+        "rg_add_edges": [P, P, _u64, _int, P],
+        "rg_del_edges": [P, P, _u64, _int, P],
+        "rg_add_pairs": [P, P, _u64, _int, P],
+        "rg_del_pairs": [P, P, _u64, _int, P],
+        "rg_get_edge_num": [P, P, _u64, P],
+        "rg_get_degrees": [P, P, P],
+        "rg_build_tree": [P, _int, _u64, P],
+        "rg_update_tree_add": [P, _int, P, _u64, _int, P],
+        "rg_update_tree_del": [P, _int, P, _u64, _int, P],
+        "rg_classify": [P, _int, P, P, _u64, _int, P],
+        "rg_apply_add": [P, _int, P, _u64, _int, P],
+        "rg_apply_del": [P, _int, P, _u64, _int, P],
+        "rg_apply_add_pairs": [P, _int, P, _u64, _int, P],
+        "rg_apply_del_pairs": [P, _int, P, _u64, _int, P],
+        "rg_get_labels": [P, P, P, P],
+        "rg_get_modified": [P, P, _u64, P],
+        "rg_clear_modified": [P],
+        "rg_value_checksum": [P, P],
+        "rg_last_stats": [P, P, P, P],
+        "rg_device_bytes": [P, P],
+        "rg_set_stream": [P, P],
+        "rg_get_stream": [P, P],
+        "rg_launch_count": [P, P],
+        "rg_profile": [P, _int],
+        "rg_profile_read": [P, P, P],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = _int
+    L.rg_status_string.argtypes = [_int]
+    L.rg_status_string.restype = ctypes.c_char_p
+    L.rg_last_error.argtypes = []
+    L.rg_last_error.restype = ctypes.c_char_p
+    for name, args, res in [
+        ("rg_gen_splitmix64", [_u64], _u64),
+        ("rg_gen_weight", [_u64, _u64], _u64),
+        ("rg_gen_rmat", [ctypes.c_uint32, _u64, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, P],
+         None),
+        ("rg_gen_er_rmat_mix",
+         [ctypes.c_uint32, _u64, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, P], None),
+        ("rg_gen_weights", [P, _u64, P], None),
+        ("rg_gen_max_out_degree_vertex", [P, _u64, _u64], _u64),
+        ("rg_gen_write_binary", [ctypes.c_char_p, P, _u64], _int),
+        ("rg_gen_value_checksum", [P, _u64], _u64),
+    ]:
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+
+
+def lib():
+    """Load librisgraph_b200.so (built in-tree by risgraph_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m risgraph_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Function names declared in a C header of include/."""
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(rg\w*)\s*\(", src, flags=re.M)
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _check(rc, where):
+    if rc != 0:
+        raise RGError(rc, where)
+
+
+def as_edges(edges) -> np.ndarray:
+    """Accept an rg_edge structured array, an (n,3) or (n,2) integer array."""
+    if isinstance(edges, np.ndarray) and edges.dtype == EDGE_DTYPE:
+        return np.ascontiguousarray(edges)
+    a = np.asarray(edges, dtype=np.uint64)
+    if a.ndim == 1:
+        a = a.reshape(1, -1)
+    out = np.zeros(a.shape[0], EDGE_DTYPE)
+    out["src"] = a[:, 0]
+    out["dst"] = a[:, 1]
+    if a.shape[1] > 2:
+        out["data"] = a[:, 2]
+    return out
+
+
+class Graph:
+    """Device-resident evolving graph with one dependency-tree label array.
+
+    Constructor arguments follow Graph(vertices, hint_edges, symmetric, dual,
+    trace_modified) of core/graph.hpp:61-100; `weighted` chooses
+    Graph<uint64_t> over Graph<void>.
+    """
+
+    def __init__(self, vertices: int, hint_edges: int = 0, symmetric: bool = False, dual: bool = True,
+                 trace_modified: bool = False, weighted: bool = False):
+        self.vertices = int(vertices)
+        self.symmetric = bool(symmetric)
+        self.weighted = bool(weighted)
+        self.trace_modified = bool(trace_modified)
+        h = ctypes.c_void_p()
+        _check(lib().rg_create(self.vertices, int(hint_edges), int(symmetric), int(dual), int(trace_modified),
+                               int(weighted), ctypes.byref(h)), "rg_create")
+        self._h = h
+        self.algo = None
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- adjacency (core/graph.hpp:198-253)
+    def _edge_op(self, fn, edges, directed, where):
+        e = as_edges(edges)
+        old = np.zeros(len(e), np.uint64)
+        _check(fn(self._h, _p(e), len(e), int(directed), _p(old)), where)
+        return old
+
+    def add_edges(self, edges, directed: bool = True) -> np.ndarray:
+        return self._edge_op(lib().rg_add_edges, edges, directed, "rg_add_edges")
+
+    def del_edges(self, edges, directed: bool = True) -> np.ndarray:
+        return self._edge_op(lib().rg_del_edges, edges, directed, "rg_del_edges")
+
+    def add_edge(self, src, dst, data=0, directed: bool = True) -> int:
+        return int(self.add_edges([(src, dst, data)], directed)[0])
+
+    def del_edge(self, src, dst, data=0, directed: bool = True) -> int:
+        return int(self.del_edges([(src, dst, data)], directed)[0])
+
+    def _pair_op(self, fn, pairs, directed, where, want_old=True):
+        p = np.ascontiguousarray(pairs, dtype=np.uint64).reshape(-1)
+        n = p.size // 2
+        old = np.zeros(n, np.uint64) if want_old else None
+        _check(fn(self._h, _p(p), n, int(directed), _p(old)), where)
+        return old
+
+    def add_pairs(self, pairs, directed: bool = True, want_old: bool = True):
+        return self._pair_op(lib().rg_add_pairs, pairs, directed, "rg_add_pairs", want_old)
+
+    def del_pairs(self, pairs, directed: bool = True, want_old: bool = True):
+        return self._pair_op(lib().rg_del_pairs, pairs, directed, "rg_del_pairs", want_old)
+
+    def get_edge_num(self, edges) -> np.ndarray:
+        e = as_edges(edges)
+        out = np.zeros(len(e), np.uint64)
+        _check(lib().rg_get_edge_num(self._h, _p(e), len(e), _p(out)), "rg_get_edge_num")
+        return out
+
+    def degrees(self):
+        o = np.zeros(self.vertices, np.uint64)
+        i = np.zeros(self.vertices, np.uint64)
+        _check(lib().rg_get_degrees(self._h, _p(o), _p(i)), "rg_get_degrees")
+        return o, i
+
+    # -- trees (core/graph.hpp:873-1718)
+    def build_tree(self, algo: str, root: int = 0) -> int:
+        tot = np.zeros(1, np.uint64)
+        _check(lib().rg_build_tree(self._h, ALGOS[algo], int(root), _p(tot)), "rg_build_tree")
+        self.algo = algo
+        return int(tot[0])
+
+    def update_tree_add(self, algo: str, edges, directed: bool = True) -> int:
+        e = as_edges(edges)
+        tot = np.zeros(1, np.uint64)
+        _check(lib().rg_update_tree_add(self._h, ALGOS[algo], _p(e), len(e), int(directed), _p(tot)),
+               "rg_update_tree_add")
+        return int(tot[0])
+
+    def update_tree_del(self, algo: str, edges, directed: bool = True) -> int:
+        e = as_edges(edges)
+        tot = np.zeros(1, np.uint64)
+        _check(lib().rg_update_tree_del(self._h, ALGOS[algo], _p(e), len(e), int(directed), _p(tot)),
+               "rg_update_tree_del")
+        return int(tot[0])
+
+    def classify(self, algo: str, edges, is_del=None, directed: bool = True) -> np.ndarray:
+        e = as_edges(edges)
+        out = np.zeros(len(e), np.uint8)
+        d = None if is_del is None else np.ascontiguousarray(is_del, dtype=np.uint8)
+        _check(lib().rg_classify(self._h, ALGOS[algo], _p(e), _p(d), len(e), int(directed), _p(out)),
+               "rg_classify")
+        return out
+
+    def need_update_tree_add(self, algo: str, edge, directed: bool = True) -> bool:
+        return bool(self.classify(algo, [edge], None, directed)[0])
+
+    def need_update_tree_del(self, algo: str, edge, directed: bool = True) -> bool:
+        return bool(self.classify(algo, [edge], np.ones(1, np.uint8), directed)[0])
+
+    def apply_add(self, algo: str, edges, directed: bool = True) -> np.ndarray:
+        return self._apply(lib().rg_apply_add, algo, as_edges(edges), directed, "rg_apply_add")
+
+    def apply_del(self, algo: str, edges, directed: bool = True) -> np.ndarray:
+        return self._apply(lib().rg_apply_del, algo, as_edges(edges), directed, "rg_apply_del")
+
+    def apply_add_pairs(self, algo: str, pairs, directed: bool = True, want_old: bool = False):
+        p = np.ascontiguousarray(pairs, dtype=np.uint64).reshape(-1)
+        return self._apply(lib().rg_apply_add_pairs, algo, p, directed, "rg_apply_add_pairs", p.size // 2, want_old)
+
+    def apply_del_pairs(self, algo: str, pairs, directed: bool = True, want_old: bool = False):
+        p = np.ascontiguousarray(pairs, dtype=np.uint64).reshape(-1)
+        return self._apply(lib().rg_apply_del_pairs, algo, p, directed, "rg_apply_del_pairs", p.size // 2, want_old)
+
+    def _apply(self, fn, algo, arr, directed, where, n=None, want_old=True):
+        n = len(arr) if n is None else n
+        old = np.zeros(n, np.uint64) if want_old else None
+        _check(fn(self._h, ALGOS[algo], _p(arr), n, int(directed), _p(old)), where)
+        return old
+
+    # -- results
+    def labels(self, value=True, parent=True, parent_w=True):
+        V = self.vertices
+        val = np.empty(V, np.uint64) if value else None
+        par = np.empty(V, np.uint64) if parent else None
+        pw = np.empty(V, np.uint64) if parent_w else None
+        _check(lib().rg_get_labels(self._h, _p(val), _p(par), _p(pw)), "rg_get_labels")
+        return val, par, pw
+
+    def values(self) -> np.ndarray:
+        return self.labels(True, False, False)[0]
+
+    def checksum(self) -> int:
+        c = np.zeros(1, np.uint64)
+        _check(lib().rg_value_checksum(self._h, _p(c)), "rg_value_checksum")
+        return int(c[0])
+
+    def get_modified(self) -> np.ndarray:
+        n = np.zeros(1, np.uint64)
+        _check(lib().rg_get_modified(self._h, None, 0, _p(n)), "rg_get_modified")
+        out = np.zeros(int(n[0]), np.uint64)
+        _check(lib().rg_get_modified(self._h, _p(out), len(out), _p(n)), "rg_get_modified")
+        return out
+
+    def clear_modified(self):
+        _check(lib().rg_clear_modified(self._h), "rg_clear_modified")
+
+    def last_stats(self):
+        a = np.zeros(3, np.uint64)
+        _check(lib().rg_last_stats(self._h, _p(a[0:1]), _p(a[1:2]), _p(a[2:3])), "rg_last_stats")
+        return {"levels": int(a[0]), "invalidated": int(a[1]), "recomputes": int(a[2])}
+
+    def set_stream(self, stream_ptr: int | None):
+        """Run this graph's work on a raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
+        _check(lib().rg_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "rg_set_stream")
+
+    def launch_count(self) -> int:
+        n = np.zeros(1, np.uint64)
+        _check(lib().rg_launch_count(self._h, _p(n)), "rg_launch_count")
+        return int(n[0])
+
+    def profile(self, enable: bool = True):
+        _check(lib().rg_profile(self._h, int(enable)), "rg_profile")
+
+    def profile_read(self):
+        n = np.zeros(1, np.uint64)
+        ms = np.zeros(1, np.float64)
+        _check(lib().rg_profile_read(self._h, _p(n), _p(ms)), "rg_profile_read")
+        return int(n[0]), float(ms[0])
+
+    def device_bytes(self) -> int:
+        b = np.zeros(1, np.uint64)
+        _check(lib().rg_device_bytes(self._h, _p(b)), "rg_device_bytes")
+        return int(b[0])
+
+
+from . import gen  # noqa: E402  (synthetic inputs; needs lib())

@@ -1,0 +1,75 @@
+"""Build recipe for librisgraph_b200.so (sm_100a) and its host tools.
+
+The shared library is built in-tree (risgraph_b200/librisgraph_b200.so) with
+explicit nvcc commands, so the same file is what loads on a GPU machine.
+Run `python -m risgraph_b200.build` or call build().
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "librisgraph_b200.so")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+HOST_CXX = "/usr/bin/g++"
+HOST_CC = "/usr/bin/gcc"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompiler", "-fPIC",
+                  "-I" + INCLUDE, "-I" + CSRC, "--expt-relaxed-constexpr"]
+
+CU_SOURCES = ["rg_api.cu", "rg_storage.cu", "rg_tree.cu"]
+C_SOURCES = ["rg_gen.c"]
+HEADERS = ["rg_internal.cuh"]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd[:3])} ...")
+    if verbose and r.stderr.strip():
+        sys.stderr.write(r.stderr)
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "risgraph_b200.h"),
+                                                       os.path.join(INCLUDE, "rg_gen.h")]
+    objs = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        if force or _newer(o, [s] + hdrs):
+            _run([NVCC] + NVFLAGS + ["-c", s, "-o", o], verbose)
+        objs.append(o)
+    for src in C_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".c", ".o"))
+        if force or _newer(o, [s] + hdrs):
+            _run([HOST_CC, "-O3", "-fPIC", "-fopenmp", "-std=c11", "-I" + INCLUDE, "-c", s, "-o", o], verbose)
+        objs.append(o)
+    if force or _newer(LIB, objs):
+        _run([NVCC] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", LIB] + objs +
+             ["-Xcompiler", "-fopenmp", "-lgomp", "-cudart", "static"], verbose)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)
+    print(LIB)

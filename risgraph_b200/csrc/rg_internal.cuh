@@ -1,0 +1,247 @@
+// Internal device layout and helpers of librisgraph_b200.
+//
+// HBM layout (per graph):
+//   labels   ulonglong2 lab[V]        {value u64, parent u32 | parent_w u32 << 32}
+//                                      parent == NONE (0xFFFFFFFF) means no parent.
+//                                      Updated as one 16-byte record with a 128-bit CAS,
+//                                      the role of the reference's 16-byte CAS / vertex lock
+//                                      in update_label (core/graph.hpp:1765-1887).
+//   adjacency, per direction (out; in unless symmetric):
+//            u64 off[V], u32 len[V], u32 cap[V], u64 deg[V]
+//            pool: weighted   uint2  {nbr | DEAD, w}
+//                  unweighted uint32  nbr | DEAD
+//            A vertex's edges are the contiguous slots [off, off+len) of the pool.
+//            DEAD marks a multiplicity-0 entry, the reference's never-compacted num==0
+//            tombstone (core/storage.hpp:391-396, skipped at core/graph.hpp:916).
+//   edge index: open-addressing table of uint4 {src, dst, w, rec} keyed by (src,dst,w)
+//            -> record rec: num (multiplicity), out slot, in slot.  One probe sequence
+//            finds an edge whatever its vertex's degree (the reference scans lists below
+//            512 entries and hashes above, core/storage.hpp:358-386).
+//   frontier queues, dedup stamps, invalidation tags, small control block.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "risgraph_b200.h"
+
+namespace rg {
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+constexpr uint32_t DEAD = 0x80000000u;
+constexpr uint32_t VID_MASK = 0x7FFFFFFFu;
+constexpr uint32_t UNSET = 0xFFFFFFFFu;
+constexpr uint64_t BFS_MAXL = 65536ull;        // src/bfs.cpp:66
+constexpr uint64_t SSSP_MAXL = 134217728ull;   // src/sssp.cpp:66, src/sswp.cpp:66
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+// Control block counters (device, u64 each).
+enum Ctl : int {
+  C_QN0 = 0,       // frontier length, queue 0
+  C_QN1 = 1,       // frontier length, queue 1
+  C_HUBN = 2,      // hub chunk tasks this level
+  C_RESULT = 3,    // successful label updates (active_result_func sum)
+  C_CANDN = 4,     // candidate edges for tree repair
+  C_TREEN = 5,     // invalidated (reset) vertices
+  C_GROWN_OUT = 6, // vertices whose out segment must grow
+  C_GROWN_IN = 7,
+  C_ERR = 8,       // first error code raised on the device
+  C_RECOMPUTE = 9, // parent-chain guard tripped (has_parents, core/graph.hpp:1900-1903)
+  C_MODN = 10,     // modified list length
+  C_CHECKSUM = 11,
+  C_AUX = 12,
+  C_COUNT = 16
+};
+
+struct DevDir {
+  uint64_t *off;
+  uint32_t *len;
+  uint32_t *cap;
+  unsigned long long *deg;
+  void *pool;
+  uint64_t pool_cap;
+  unsigned long long *pool_top;
+  uint32_t *grow;   // vertices to grow
+};
+
+struct DevGraph {
+  uint32_t V;
+  int weighted, symmetric;
+  DevDir out, in;
+  ulonglong2 *ht;
+  uint64_t ht_mask;
+  uint32_t *rec_num, *rec_out, *rec_in;
+  unsigned long long *rec_top;
+  uint64_t rec_cap;
+  ulonglong2 *lab;
+  uint32_t *stamp;
+  uint32_t *inv;
+  uint32_t *modstamp;
+  uint32_t *modq;
+  unsigned long long *ctl;
+};
+
+// ---- per-algorithm hooks (a8): update_func = better(combine(s,w), d);
+//      equal_func = combine(s,w) == d; init_label_func = init/active. ----
+template <int A>
+struct Hook;
+template <>
+struct Hook<RG_BFS> {  // src/bfs.cpp:76-91
+  static __host__ __device__ __forceinline__ uint64_t combine(uint64_t s, uint64_t) { return s + 1; }
+  static __host__ __device__ __forceinline__ bool better(uint64_t a, uint64_t b) { return a < b; }
+  static __host__ __device__ __forceinline__ uint64_t init(uint64_t v, uint64_t r) { return v == r ? 0 : BFS_MAXL; }
+  static constexpr bool all_active = false;
+};
+template <>
+struct Hook<RG_SSSP> {  // src/sssp.cpp:67-91
+  static __host__ __device__ __forceinline__ uint64_t combine(uint64_t s, uint64_t w) { return s + w; }
+  static __host__ __device__ __forceinline__ bool better(uint64_t a, uint64_t b) { return a < b; }
+  static __host__ __device__ __forceinline__ uint64_t init(uint64_t v, uint64_t r) { return v == r ? 0 : SSSP_MAXL; }
+  static constexpr bool all_active = false;
+};
+template <>
+struct Hook<RG_SSWP> {  // src/sswp.cpp:76-91
+  static __host__ __device__ __forceinline__ uint64_t combine(uint64_t s, uint64_t w) { return s < w ? s : w; }
+  static __host__ __device__ __forceinline__ bool better(uint64_t a, uint64_t b) { return a > b; }
+  static __host__ __device__ __forceinline__ uint64_t init(uint64_t v, uint64_t r) { return v == r ? SSSP_MAXL : 0; }
+  static constexpr bool all_active = false;
+};
+template <>
+struct Hook<RG_WCC> {  // src/wcc.cpp:62-86
+  static __host__ __device__ __forceinline__ uint64_t combine(uint64_t s, uint64_t) { return s; }
+  static __host__ __device__ __forceinline__ bool better(uint64_t a, uint64_t b) { return a < b; }
+  static __host__ __device__ __forceinline__ uint64_t init(uint64_t v, uint64_t) { return v; }
+  static constexpr bool all_active = true;
+};
+
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ uint64_t pack_parent(uint32_t p, uint32_t w) {
+  return (uint64_t)p | ((uint64_t)w << 32);
+}
+
+// ---- memory access helpers ----
+__device__ __forceinline__ ulonglong2 cas128(ulonglong2 *addr, ulonglong2 cmp, ulonglong2 val) {
+  ulonglong2 old;
+  asm volatile(
+      "{\n\t.reg .b128 d, b, c;\n\t"
+      "mov.b128 b, {%2, %3};\n\t"
+      "mov.b128 c, {%4, %5};\n\t"
+      "atom.relaxed.gpu.global.cas.b128 d, [%6], b, c;\n\t"
+      "mov.b128 {%0, %1}, d;\n\t}"
+      : "=l"(old.x), "=l"(old.y)
+      : "l"(cmp.x), "l"(cmp.y), "l"(val.x), "l"(val.y), "l"(addr)
+      : "memory");
+  return old;
+}
+
+// Coherent (L2) 16-byte load: labels are written by other SMs inside a launch.
+__device__ __forceinline__ ulonglong2 ld_lab(const ulonglong2 *p) { return __ldcg(p); }
+__device__ __forceinline__ uint64_t ld_val(const ulonglong2 *p) {
+  return __ldcg(reinterpret_cast<const unsigned long long *>(p));
+}
+__device__ __forceinline__ uint64_t ld_meta(const ulonglong2 *p) {
+  return __ldcg(reinterpret_cast<const unsigned long long *>(p) + 1);
+}
+__device__ __forceinline__ uint32_t ld_u32(const uint32_t *p) { return __ldcg(p); }
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Warp-aggregated append of `v` by every lane with pred set (all lanes of mask
+// must call).  Returns nothing; writes q[base + rank].
+__device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t *q, unsigned long long *cnt,
+                                            unsigned mask) {
+  unsigned b = __ballot_sync(mask, pred);
+  if (!b) return;
+  int leader = __ffs(b) - 1;
+  unsigned long long base = 0;
+  if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(b));
+  base = __shfl_sync(mask, base, leader);
+  if (pred) q[base + __popc(b & ((1u << lane_id()) - 1))] = v;
+}
+
+// ---- host-side graph object ----
+struct Graph {
+  DevGraph d{};
+  uint64_t V = 0, hint = 0;
+  int symmetric = 0, dual = 1, trace = 0, weighted = 0;
+  int algo = -1;
+  uint64_t root = 0;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int num_sms = 148;
+  // frontier queues (V entries each)
+  uint32_t *q[2] = {nullptr, nullptr};
+  uint32_t *tree = nullptr;   // invalidated set
+  uint64_t *hubq = nullptr;   // hub chunk tasks (vertex | chunk << 32)
+  uint64_t hubq_cap = 0;
+  // staging for update batches
+  void *stage_dev = nullptr;
+  size_t stage_dev_bytes = 0;
+  void *stage_host = nullptr;  // pinned
+  size_t stage_host_bytes = 0;
+  uint32_t *ops = nullptr;     // s,d,w,rid,old... per directed op (SoA inside)
+  uint64_t ops_cap = 0;
+  unsigned long long *h_ctl = nullptr;  // pinned mirror of ctl
+  uint32_t stamp_epoch = 0;
+  uint32_t inv_epoch = 0;
+  uint32_t mod_epoch = 1;
+  uint64_t *scratch64 = nullptr;  // V u64 (unpack labels, checksums)
+  // stats of the last tree call
+  uint64_t st_levels = 0, st_invalidated = 0, st_recomputes = 0;
+  uint64_t bytes = 0;
+  std::string err;
+  cudaStream_t own_stream = nullptr;
+  // kernel accounting
+  uint64_t launches = 0;
+  int profiling = 0;
+  cudaEvent_t pev[2] = {nullptr, nullptr};
+  uint64_t prof_launches = 0;
+  double prof_ms = 0.0;
+};
+
+// Kernel launch bookkeeping (every launch site calls count_launch).
+inline void count_launch(Graph &g, int n = 1) { g.launches += (uint64_t)n; }
+
+// Error plumbing (thread-local last error message).
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define RG_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t _e = (call);                           \
+    if (_e != cudaSuccess) return rg::cuda_fail(_e, #call); \
+  } while (0)
+
+// ---- storage (rg_storage.cu) ----
+int storage_alloc(Graph &g);
+void storage_free(Graph &g);
+// Stage n edges (rg_edge or reference pairs) into the device op arrays as
+// directed ops (2 per edge when undirected).  Returns number of ops.
+int stage_edges(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, uint64_t *nops);
+int storage_add(Graph &g, uint64_t n_edges, uint64_t nops, int directed, uint64_t *old_num, bool collect);
+int storage_del(Graph &g, uint64_t n_edges, uint64_t nops, int directed, uint64_t *old_num, bool collect);
+int storage_num(Graph &g, uint64_t nops, uint64_t *num);
+// op array accessors (device pointers)
+uint32_t *op_src(Graph &g);
+uint32_t *op_dst(Graph &g);
+uint32_t *op_w(Graph &g);
+uint32_t *op_cand(Graph &g);   // candidate edge indices after storage_add/del(collect)
+
+// ---- trees (rg_tree.cu) ----
+int tree_build(Graph &g, int algo, uint64_t root, uint64_t *total);
+// Repair for candidate edges: edges [0,n) given as staged ops (cands == nullptr:
+// all staged edges are candidates; else indices in op_cand with count in ctl).
+int tree_add(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total);
+int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total);
+int tree_classify(Graph &g, uint64_t n_edges, int directed, const uint8_t *is_del_dev, uint8_t *unsafe_dev);
+int tree_labels(Graph &g, uint64_t *val, uint64_t *par, uint64_t *pw);
+int tree_checksum(Graph &g, uint64_t *sum);
+int tree_alloc(Graph &g);
+
+}  // namespace rg

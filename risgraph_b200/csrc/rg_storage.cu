@@ -1,0 +1,515 @@
+// Device-resident dynamic adjacency with multiplicity counts: the B200 form of
+// the reference's IndexedEdgeStorage (core/storage.hpp:282-430) and of
+// Graph::add_edge / del_edge (core/graph.hpp:203-253).
+//
+// A batch of edge updates runs as a short fixed sequence of kernels with no host
+// decision in between:
+//   unpack   -> directed ops (two per undirected edge, as add_edge(e,false) does)
+//   lookup   -> find (src,dst,w) in the edge index, creating the record and
+//               reserving a slot at the end of the src (and dst) segment if new
+//   grow     -> move segments that ran out of capacity to a larger pool region
+//   write    -> store the new entries, still DEAD (multiplicity 0)
+//   count    -> atomic multiplicity update returning the old count; the 0->1
+//               and 1->0 transitions flip the DEAD bit
+//   edge_old -> per-edge old count with the reference's undirected conventions,
+//               plus the candidate list for tree repair (0->1 adds, 1->0 dels)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "rg_internal.cuh"
+
+namespace rg {
+
+namespace {
+
+constexpr int TPB = 256;
+
+// O_MUL: multiplicity delta of the op (1; 2 for an undirected self-loop, whose
+// two add_edge calls hit the same key; 0 = no-op).
+enum OpArr { O_SRC = 0, O_DST, O_W, O_RID, O_OLD, O_MUL, O_SPARE, O_FLAG, O_NARR };
+
+struct OpView {
+  uint32_t *src, *dst, *w, *rid, *old, *mul, *spare, *flag;
+};
+
+__device__ __forceinline__ uint64_t ht_hash(uint32_t s, uint32_t d, uint32_t w) {
+  return splitmix64(((uint64_t)s << 32 | d) ^ splitmix64((uint64_t)w + 0x5851F42D4C957F2Dull));
+}
+
+__device__ __forceinline__ void set_err(unsigned long long *ctl, int code) {
+  atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)code);
+}
+
+// Directed ops of edge i: one when directed; (s,d) and (d,s) when undirected
+// (add_edge(e,false), core/graph.hpp:206-211).  An undirected self-loop is a
+// single op of delta 2 on its one key, so concurrent duplicates still see a
+// serial sequence of counts.
+__device__ __forceinline__ void put_ops(OpView ops, uint64_t i, uint32_t s, uint32_t d, uint32_t w, int directed) {
+  if (directed) {
+    ops.src[i] = s; ops.dst[i] = d; ops.w[i] = w; ops.mul[i] = 1;
+  } else {
+    ops.src[2 * i] = s; ops.dst[2 * i] = d; ops.w[2 * i] = w; ops.mul[2 * i] = s == d ? 2 : 1;
+    ops.src[2 * i + 1] = d; ops.dst[2 * i + 1] = s; ops.w[2 * i + 1] = w; ops.mul[2 * i + 1] = s == d ? 0 : 1;
+  }
+}
+
+__global__ void k_unpack_edges(const rg_edge *e, uint64_t n, int directed, int weighted, OpView ops) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t s = (uint32_t)e[i].src, d = (uint32_t)e[i].dst, w = weighted ? (uint32_t)e[i].data : 0u;
+    put_ops(ops, i, s, d, w, directed);
+  }
+}
+
+// Reference file format pairs; weights are the pure function of the endpoints
+// used by every implementation here (splitmix64(src<<32|dst) % 255 + 1).
+__global__ void k_unpack_pairs(const uint64_t *p, uint64_t n, int directed, int weighted, OpView ops) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint64_t s64 = p[2 * i], d64 = p[2 * i + 1];
+    uint32_t s = (uint32_t)s64, d = (uint32_t)d64;
+    uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
+    put_ops(ops, i, s, d, w, directed);
+  }
+}
+
+// Find the record of (s,d,w); create it (and reserve its slots) when `create`.
+__global__ void k_lookup(DevGraph g, OpView ops, uint64_t nops, int create) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nops; j += stride) {
+    uint32_t s = ops.src[j], d = ops.dst[j], w = ops.w[j];
+    if (ops.mul[j] == 0) { ops.rid[j] = UNSET; ops.flag[j] = 0; continue; }
+    ulonglong2 key = make_ulonglong2((uint64_t)s | ((uint64_t)d << 32), (uint64_t)w);
+    uint64_t h = ht_hash(s, d, w) & g.ht_mask;
+    uint32_t rid = UNSET, mine = UNSET;
+    int created = 0;
+    for (uint64_t probe = 0; probe <= g.ht_mask; probe++) {
+      ulonglong2 e = __ldcg(&g.ht[h]);
+      if ((uint32_t)e.x == NONE) {
+        if (!create) break;
+        if (mine == UNSET) {
+          unsigned long long r = atomicAdd(g.rec_top, 1ull);
+          if (r >= g.rec_cap) { set_err(g.ctl, RG_ENOSPACE); break; }
+          mine = (uint32_t)r;
+          g.rec_num[mine] = 0;
+          g.rec_out[mine] = UNSET;
+          g.rec_in[mine] = UNSET;
+          __threadfence();
+        }
+        ulonglong2 want = make_ulonglong2(key.x, key.y | ((uint64_t)mine << 32));
+        ulonglong2 old = cas128(&g.ht[h], make_ulonglong2(~0ull, ~0ull), want);
+        if (old.x == ~0ull && old.y == ~0ull) { rid = mine; created = 1; break; }
+        e = old;
+      }
+      // A 16-byte load racing with the claiming CAS may see the new (src,dst)
+      // half with the old (all-ones) half; re-read atomically before deciding.
+      if (e.x == key.x && (uint32_t)e.y != w) e = cas128(&g.ht[h], make_ulonglong2(~0ull, ~0ull), make_ulonglong2(~0ull, ~0ull));
+      if (e.x == key.x && (uint32_t)e.y == w) { rid = (uint32_t)(e.y >> 32); break; }
+      h = (h + 1) & g.ht_mask;
+    }
+    if (create && rid == UNSET && mine == UNSET) set_err(g.ctl, RG_ENOSPACE);
+    ops.rid[j] = rid;
+    ops.flag[j] = created;
+    if (created) {
+      uint32_t po = atomicAdd(&g.out.len[s], 1u);
+      g.rec_out[rid] = po;
+      if (po == g.out.cap[s]) {
+        unsigned long long k = atomicAdd(&g.ctl[C_GROWN_OUT], 1ull);
+        g.out.grow[k] = s;
+      }
+      if (!g.symmetric) {
+        uint32_t pi = atomicAdd(&g.in.len[d], 1u);
+        g.rec_in[rid] = pi;
+        if (pi == g.in.cap[d]) {
+          unsigned long long k = atomicAdd(&g.ctl[C_GROWN_IN], 1ull);
+          g.in.grow[k] = d;
+        }
+      }
+    }
+  }
+}
+
+// One CTA per growing vertex: new region from the pool bump pointer, copy the
+// existing slots.  Initial loads (cap 0) get exactly len + len/8 + 2.
+template <bool W>
+__global__ void k_grow(DevDir dir, unsigned long long *ctl, int which) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *pool = reinterpret_cast<E *>(dir.pool);
+  unsigned long long n = ctl[which];
+  __shared__ uint64_t s_new_off;
+  __shared__ uint32_t s_copy, s_new_cap;
+  for (unsigned long long k = blockIdx.x; k < n; k += gridDim.x) {
+    uint32_t v = dir.grow[k];
+    if (threadIdx.x == 0) {
+      uint32_t len = dir.len[v], cap = dir.cap[v];
+      uint64_t want = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
+      while (want < len) want *= 2;
+      if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
+      unsigned long long off = atomicAdd(dir.pool_top, (unsigned long long)want);
+      if (off + want > dir.pool_cap) {
+        atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
+        s_new_cap = 0;
+      } else {
+        s_new_cap = (uint32_t)want;
+      }
+      s_new_off = off;
+      s_copy = len < cap ? len : cap;
+    }
+    __syncthreads();
+    if (s_new_cap) {
+      uint64_t from = dir.off[v];
+      for (uint32_t i = threadIdx.x; i < s_copy; i += blockDim.x) pool[s_new_off + i] = pool[from + i];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        dir.off[v] = s_new_off;
+        dir.cap[v] = s_new_cap;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <bool W>
+__global__ void k_write_new(DevGraph g, OpView ops, uint64_t nops) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *po = reinterpret_cast<E *>(g.out.pool);
+  E *pi = reinterpret_cast<E *>(g.in.pool);
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nops; j += stride) {
+    if (!ops.flag[j]) continue;
+    uint32_t s = ops.src[j], d = ops.dst[j], w = ops.w[j], rid = ops.rid[j];
+    uint32_t ps = g.rec_out[rid];
+    if (ps < g.out.cap[s]) {
+      if constexpr (W) po[g.out.off[s] + ps] = make_uint2(d | DEAD, w);
+      else po[g.out.off[s] + ps] = d | DEAD;
+    }
+    if (!g.symmetric) {
+      uint32_t pd = g.rec_in[rid];
+      if (pd < g.in.cap[d]) {
+        if constexpr (W) pi[g.in.off[d] + pd] = make_uint2(s | DEAD, w);
+        else pi[g.in.off[d] + pd] = s | DEAD;
+      }
+    }
+  }
+}
+
+template <bool W>
+__device__ __forceinline__ void set_alive(DevDir &dir, uint32_t v, uint32_t pos, uint32_t nbr, bool alive) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *pool = reinterpret_cast<E *>(dir.pool);
+  if (pos >= dir.cap[v]) return;
+  uint32_t x = alive ? nbr : (nbr | DEAD);
+  if constexpr (W) reinterpret_cast<uint32_t *>(&pool[dir.off[v] + pos])[0] = x;
+  else pool[dir.off[v] + pos] = x;
+}
+
+template <bool W>
+__global__ void k_count(DevGraph g, OpView ops, uint64_t nops, int add) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nops; j += stride) {
+    uint32_t rid = ops.rid[j];
+    uint32_t s = ops.src[j], d = ops.dst[j];
+    if (rid == UNSET) { ops.old[j] = 0; continue; }
+    const uint32_t mul = ops.mul[j];
+    uint32_t old;
+    if (add) {
+      // update_edge(+1) (core/storage.hpp:390-396), mul times
+      old = atomicAdd(&g.rec_num[rid], mul);
+      atomicAdd(&g.out.deg[s], (unsigned long long)mul);
+      if (!g.symmetric) atomicAdd(&g.in.deg[d], (unsigned long long)mul);
+      if (old == 0) {
+        set_alive<W>(g.out, s, g.rec_out[rid], d, true);
+        if (!g.symmetric) set_alive<W>(g.in, d, g.rec_in[rid], s, true);
+      }
+    } else {
+      // update_edge(-1): the count never goes below zero
+      old = g.rec_num[rid];
+      while (old > 0) {
+        uint32_t nv = old >= mul ? old - mul : 0u;
+        uint32_t seen = atomicCAS(&g.rec_num[rid], old, nv);
+        if (seen == old) break;
+        old = seen;
+      }
+      uint32_t dropped = old < mul ? old : mul;
+      if (dropped) {
+        atomicAdd(&g.out.deg[s], 0ull - dropped);
+        if (!g.symmetric) atomicAdd(&g.in.deg[d], 0ull - dropped);
+      }
+      if (old != 0 && old <= mul) {
+        set_alive<W>(g.out, s, g.rec_out[rid], d, false);
+        if (!g.symmetric) set_alive<W>(g.in, d, g.rec_in[rid], s, false);
+      }
+    }
+    ops.old[j] = old;
+  }
+}
+
+// Per-edge old multiplicity with add_edge/del_edge's undirected conventions
+// (core/graph.hpp:206-211: second orientation's count, minus one for a
+// self-loop on add; :232-237 for delete) and the tree-repair candidates:
+// 0->1 adds (src/sssp_inc_batch.cpp:148) and 1->0 deletes (:166).
+__global__ void k_edge_old(OpView ops, uint64_t n, int directed, int add, int collect, uint64_t *old_out,
+                           uint32_t *cand, unsigned long long *ctl) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t o;
+    if (directed) {
+      o = ops.old[i];
+    } else {
+      const uint32_t s = ops.src[2 * i], d = ops.dst[2 * i];
+      if (s == d) {
+        // add returns old+1-1, delete the second call's old (max(old-1,0))
+        uint32_t a = ops.old[2 * i];
+        o = add ? a : (a ? a - 1 : 0);
+      } else {
+        // both orientations move together; the canonical (lower src) key gives a
+        // serial count sequence even when (s,d) and (d,s) share a batch
+        o = ops.old[2 * i + (s < d ? 0 : 1)];
+      }
+    }
+    if (old_out) old_out[i] = o;
+    if (collect && (add ? o == 0 : o == 1)) {
+      unsigned long long k = atomicAdd(&ctl[C_CANDN], 1ull);
+      cand[k] = (uint32_t)i;
+    }
+  }
+}
+
+__global__ void k_get_num(DevGraph g, OpView ops, uint64_t nops, uint64_t *out) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nops; j += stride) {
+    uint32_t rid = ops.rid[j];
+    out[j] = rid == UNSET ? 0 : g.rec_num[rid];
+  }
+}
+
+OpView op_view(Graph &g) {
+  OpView v;
+  uint32_t **f = reinterpret_cast<uint32_t **>(&v);
+  for (int i = 0; i < O_NARR; i++) f[i] = g.ops + (uint64_t)i * g.ops_cap;
+  return v;
+}
+
+int grid_for(const Graph &g, uint64_t n) {
+  uint64_t b = (n + TPB - 1) / TPB;
+  uint64_t cap = (uint64_t)g.num_sms * 16;
+  if (b > cap) b = cap;
+  if (b == 0) b = 1;
+  return (int)b;
+}
+
+int ensure_ops(Graph &g, uint64_t nops, uint64_t n_edges) {
+  if (nops <= g.ops_cap && g.ops) return RG_OK;
+  uint64_t cap = std::max<uint64_t>(nops, 1024);
+  cap = std::max<uint64_t>(cap, g.ops_cap * 2);
+  cap = (cap + 63) & ~63ull;  // keeps the u64 old-count array 8-byte aligned
+  if (g.ops) cudaFree(g.ops);
+  g.ops = nullptr;
+  // O_NARR u32 arrays + candidate list (n_edges u32) + u64 old per edge
+  size_t bytes = (size_t)cap * (O_NARR + 1) * 4 + (size_t)cap * 8;
+  cudaError_t e = cudaMalloc(&g.ops, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(ops)");
+  g.ops_cap = cap;
+  (void)n_edges;
+  return RG_OK;
+}
+
+int ensure_stage(Graph &g, size_t bytes) {
+  if (bytes > g.stage_dev_bytes) {
+    if (g.stage_dev) cudaFree(g.stage_dev);
+    g.stage_dev = nullptr;
+    size_t b = std::max(bytes, g.stage_dev_bytes * 2);
+    cudaError_t e = cudaMalloc(&g.stage_dev, b);
+    if (e != cudaSuccess) { g.stage_dev_bytes = 0; return cuda_fail(e, "cudaMalloc(stage)"); }
+    g.stage_dev_bytes = b;
+  }
+  if (bytes > g.stage_host_bytes) {
+    if (g.stage_host) cudaFreeHost(g.stage_host);
+    g.stage_host = nullptr;
+    size_t b = std::max(bytes, g.stage_host_bytes * 2);
+    cudaError_t e = cudaHostAlloc(&g.stage_host, b, cudaHostAllocDefault);
+    if (e != cudaSuccess) { g.stage_host_bytes = 0; return cuda_fail(e, "cudaHostAlloc(stage)"); }
+    g.stage_host_bytes = b;
+  }
+  return RG_OK;
+}
+
+uint64_t *old_dev(Graph &g) {
+  return reinterpret_cast<uint64_t *>(g.ops + (uint64_t)(O_NARR + 1) * g.ops_cap);
+}
+
+// Read the device error word; also syncs the stream.
+int finish(Graph &g, bool need_old, uint64_t *old_num, uint64_t n) {
+  RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT, cudaMemcpyDeviceToHost, g.stream));
+  if (need_old && old_num)
+    RG_CUDA(cudaMemcpyAsync(old_num, old_dev(g), n * 8, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  if (g.h_ctl[C_ERR]) {
+    int code = (int)g.h_ctl[C_ERR];
+    set_error(code == RG_ENOSPACE ? "device edge pool or edge index is full" : "device error");
+    cudaMemsetAsync(&g.d.ctl[C_ERR], 0, 8, g.stream);
+    return code;
+  }
+  return RG_OK;
+}
+
+}  // namespace
+
+uint32_t *op_src(Graph &g) { return g.ops + (uint64_t)O_SRC * g.ops_cap; }
+uint32_t *op_dst(Graph &g) { return g.ops + (uint64_t)O_DST * g.ops_cap; }
+uint32_t *op_w(Graph &g) { return g.ops + (uint64_t)O_W * g.ops_cap; }
+uint32_t *op_cand(Graph &g) { return g.ops + (uint64_t)O_NARR * g.ops_cap; }
+
+static uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+int storage_alloc(Graph &g) {
+  uint64_t V = g.V;
+  uint64_t keys = g.hint * (g.symmetric ? 2 : 1);
+  if (keys < 1024) keys = 1024;
+  uint64_t ht_cap = next_pow2(keys + keys / 2);  // load <= 2/3 at the hint
+  uint64_t rec_cap = ht_cap - ht_cap / 8;
+  uint64_t pool_cap = keys + keys / 2 + 8 * V + 1024;  // slack for growth
+  size_t esz = g.weighted ? 8 : 4;
+  auto alloc = [&](void **p, size_t bytes, const char *what) -> int {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(std::string("device allocation failed: ") + what);
+      return RG_ENOMEM_HBM;
+    }
+    g.bytes += bytes;
+    return RG_OK;
+  };
+  int rc;
+  DevGraph &d = g.d;
+  d.V = (uint32_t)V;
+  d.weighted = g.weighted;
+  d.symmetric = g.symmetric;
+  for (int dir = 0; dir < (g.symmetric ? 1 : 2); dir++) {
+    DevDir &D = dir == 0 ? d.out : d.in;
+    if ((rc = alloc((void **)&D.off, V * 8 + 8, "segment offsets"))) return rc;
+    if ((rc = alloc((void **)&D.len, V * 4 + 4, "segment lengths"))) return rc;
+    if ((rc = alloc((void **)&D.cap, V * 4 + 4, "segment capacities"))) return rc;
+    if ((rc = alloc((void **)&D.deg, V * 8 + 8, "degrees"))) return rc;
+    if ((rc = alloc((void **)&D.grow, V * 4 + 4, "grow list"))) return rc;
+    if ((rc = alloc(&D.pool, pool_cap * esz, "edge pool"))) return rc;
+    if ((rc = alloc((void **)&D.pool_top, 8, "pool top"))) return rc;
+    D.pool_cap = pool_cap;
+    RG_CUDA(cudaMemset(D.off, 0, V * 8 + 8));
+    RG_CUDA(cudaMemset(D.len, 0, V * 4 + 4));
+    RG_CUDA(cudaMemset(D.cap, 0, V * 4 + 4));
+    RG_CUDA(cudaMemset(D.deg, 0, V * 8 + 8));
+    RG_CUDA(cudaMemset(D.pool_top, 0, 8));
+  }
+  if (g.symmetric) d.in = d.out;  // incoming == outgoing (core/graph.hpp:167,183,194)
+  if ((rc = alloc((void **)&d.ht, ht_cap * 16, "edge index"))) return rc;
+  RG_CUDA(cudaMemset(d.ht, 0xff, ht_cap * 16));
+  d.ht_mask = ht_cap - 1;
+  if ((rc = alloc((void **)&d.rec_num, rec_cap * 4, "edge records"))) return rc;
+  if ((rc = alloc((void **)&d.rec_out, rec_cap * 4, "edge records"))) return rc;
+  if ((rc = alloc((void **)&d.rec_in, rec_cap * 4, "edge records"))) return rc;
+  if ((rc = alloc((void **)&d.rec_top, 8, "record top"))) return rc;
+  RG_CUDA(cudaMemset(d.rec_top, 0, 8));
+  d.rec_cap = rec_cap;
+  return RG_OK;
+}
+
+void storage_free(Graph &g) {
+  DevGraph &d = g.d;
+  for (int dir = 0; dir < (g.symmetric ? 1 : 2); dir++) {
+    DevDir &D = dir == 0 ? d.out : d.in;
+    cudaFree(D.off); cudaFree(D.len); cudaFree(D.cap); cudaFree(D.deg); cudaFree(D.grow);
+    cudaFree(D.pool); cudaFree(D.pool_top);
+  }
+  cudaFree(d.ht); cudaFree(d.rec_num); cudaFree(d.rec_out); cudaFree(d.rec_in); cudaFree(d.rec_top);
+  if (g.ops) cudaFree(g.ops);
+  if (g.stage_dev) cudaFree(g.stage_dev);
+  if (g.stage_host) cudaFreeHost(g.stage_host);
+  g.ops = nullptr; g.stage_dev = nullptr; g.stage_host = nullptr;
+}
+
+int stage_edges(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, uint64_t *nops) {
+  uint64_t k = directed ? n : 2 * n;
+  *nops = k;
+  int rc = ensure_ops(g, k, n);
+  if (rc) return rc;
+  size_t bytes = pairs ? n * 16 : n * sizeof(rg_edge);
+  if ((rc = ensure_stage(g, bytes))) return rc;
+  if (n == 0) return RG_OK;
+  std::memcpy(g.stage_host, pairs ? (const void *)pairs : (const void *)edges, bytes);
+  RG_CUDA(cudaMemcpyAsync(g.stage_dev, g.stage_host, bytes, cudaMemcpyHostToDevice, g.stream));
+  OpView ops = op_view(g);
+  count_launch(g);
+  if (pairs)
+    k_unpack_pairs<<<grid_for(g, n), TPB, 0, g.stream>>>((const uint64_t *)g.stage_dev, n, directed, g.weighted, ops);
+  else
+    k_unpack_edges<<<grid_for(g, n), TPB, 0, g.stream>>>((const rg_edge *)g.stage_dev, n, directed, g.weighted, ops);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
+}
+
+static int grow_dir(Graph &g, DevDir &dir, int which) {
+  int grid = g.num_sms * 8;
+  count_launch(g);
+  if (g.weighted) k_grow<true><<<grid, TPB, 0, g.stream>>>(dir, g.d.ctl, which);
+  else k_grow<false><<<grid, TPB, 0, g.stream>>>(dir, g.d.ctl, which);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
+}
+
+int storage_add(Graph &g, uint64_t n, uint64_t nops, int directed, uint64_t *old_num, bool collect) {
+  OpView ops = op_view(g);
+  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_GROWN_OUT], 0, 16, g.stream));
+  if (collect) RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_CANDN], 0, 8, g.stream));
+  if (nops) {
+    count_launch(g, 4);
+    k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
+    RG_CUDA(cudaGetLastError());
+    int rc = grow_dir(g, g.d.out, C_GROWN_OUT);
+    if (rc) return rc;
+    if (!g.symmetric && (rc = grow_dir(g, g.d.in, C_GROWN_IN))) return rc;
+    if (g.weighted) {
+      k_write_new<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
+      k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
+    } else {
+      k_write_new<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
+      k_count<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
+    }
+    k_edge_old<<<grid_for(g, n), TPB, 0, g.stream>>>(ops, n, directed, 1, collect, old_dev(g), op_cand(g), g.d.ctl);
+    RG_CUDA(cudaGetLastError());
+  }
+  return finish(g, true, old_num, n);
+}
+
+int storage_del(Graph &g, uint64_t n, uint64_t nops, int directed, uint64_t *old_num, bool collect) {
+  OpView ops = op_view(g);
+  if (collect) RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_CANDN], 0, 8, g.stream));
+  if (nops) {
+    count_launch(g, 3);
+    k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+    if (g.weighted) k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+    else k_count<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+    k_edge_old<<<grid_for(g, n), TPB, 0, g.stream>>>(ops, n, directed, 0, collect, old_dev(g), op_cand(g), g.d.ctl);
+    RG_CUDA(cudaGetLastError());
+  }
+  return finish(g, true, old_num, n);
+}
+
+int storage_num(Graph &g, uint64_t nops, uint64_t *num) {
+  OpView ops = op_view(g);
+  if (nops) {
+    count_launch(g, 2);
+    k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+    k_get_num<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, old_dev(g));
+    RG_CUDA(cudaGetLastError());
+  }
+  return finish(g, true, num, nops);
+}
+
+}  // namespace rg

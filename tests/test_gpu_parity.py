@@ -1,0 +1,310 @@
+"""CUDA path vs the oracle, through the C ABI: values bit-exact, parents checked
+structurally (they are race-dependent in the reference too)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import risgraph_b200 as rg
+from risgraph_b200 import gen
+
+from helpers import ALGOS, WEIGHTED, edges_of, gpu_graph, oracle_graph
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def check_tree(g, og, root=0):
+    val, par, pw = g.labels()
+    r = og.validate(val, par, pw, root)
+    assert r == 0, f"invalid dependency tree at vertex/kind {r}"
+    return val
+
+
+# ---------------------------------------------------------------- full build
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("scale", [10, 14])
+def test_build_tree_parity(algo, scale):
+    pairs = gen.rmat(scale, seed=11)
+    V = 1 << scale
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = gpu_graph(algo, V, pairs)
+    og = oracle_graph(algo, V, pairs)
+    g.build_tree(algo, root)
+    og.build_tree(root)
+    val = check_tree(g, og, root)
+    np.testing.assert_array_equal(val, og.labels()[0])
+    # idempotent: a second build gives the same values
+    g.build_tree(algo, root)
+    np.testing.assert_array_equal(g.values(), val)
+
+
+@pytest.mark.parametrize("name", [n for n in json.load(open(os.path.join(GOLDEN, "index.json")))])
+def test_golden_reference_fixtures(name):
+    """Against values and per-step checksums produced by the reference itself."""
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    m = json.loads(str(z["meta"]))
+    pairs = gen.rmat(m["scale"], seed=m["seed"])
+    algo, V, root = m["algo"], m["V"], m["root"]
+    directed = algo != "wcc"
+    if m["mode"] == "build":
+        g = gpu_graph(algo, V, pairs)
+        g.build_tree(algo, root)
+    else:
+        imported = int(len(pairs) * m["rate"])
+        g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs), inc_mode=True)
+        g.build_tree(algo, root)
+        sums = []
+        if m["mode"] == "inc":
+            for i in range(imported, imported + m["steps"]):
+                g.apply_add_pairs(algo, pairs[i:i + 1], directed)
+                g.apply_del_pairs(algo, pairs[i - imported:i - imported + 1], directed)
+                sums.append(g.checksum())
+        else:
+            b = m["batch"]
+            for k in range(m["nbatches"]):
+                lo = imported + k * b
+                hi = min(lo + b, len(pairs))
+                g.apply_add_pairs(algo, pairs[lo:hi], directed)
+                g.apply_del_pairs(algo, pairs[lo - imported:hi - imported], directed)
+                sums.append(g.checksum())
+        np.testing.assert_array_equal(np.array(sums, np.uint64), z["sums"])
+    np.testing.assert_array_equal(g.values(), z["val"])
+
+
+# ------------------------------------------------------- incremental, single
+@pytest.mark.parametrize("algo", ALGOS)
+def test_inc_single_updates_vs_oracle(algo):
+    """bfs_inc-style sliding window: insert raw[i], delete raw[i-imported], each
+    repaired immediately; value checksum compared after every step."""
+    scale, steps = 14, 1500
+    pairs = gen.rmat(scale, seed=5)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs), inc_mode=True)
+    og = oracle_graph(algo, V, pairs[:imported], inc_mode=True)
+    g.build_tree(algo, 0)
+    og.build_tree(0)
+    ref = og.run_inc(pairs, imported, steps, 0)
+    directed = algo != "wcc"
+    for k in range(steps):
+        i = imported + k
+        g.apply_add_pairs(algo, pairs[i:i + 1], directed)
+        g.apply_del_pairs(algo, pairs[k:k + 1], directed)
+        assert g.checksum() == int(ref[k]), f"step {k}"
+    val = check_tree(g, og)
+    np.testing.assert_array_equal(val, og.labels()[0])
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_reference_api_sequence(algo):
+    """The driver sequence with host decisions (src/sssp_inc.cpp:295-324):
+    add_edge -> if old==0 update_tree_add; del_edge -> if old==1 update_tree_del."""
+    scale, steps = 12, 300
+    pairs = gen.rmat(scale, seed=9)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs), inc_mode=True)
+    og = oracle_graph(algo, V, pairs[:imported], inc_mode=True)
+    g.build_tree(algo, 0)
+    og.build_tree(0)
+    ref = og.run_inc(pairs, imported, steps, 0)
+    directed = algo != "wcc"
+    e_all = edges_of(algo, pairs)
+    for k in range(steps):
+        e = e_all[imported + k:imported + k + 1]
+        if g.add_edges(e, directed)[0] == 0:
+            g.update_tree_add(algo, e, directed)
+        e = e_all[k:k + 1]
+        if g.del_edges(e, directed)[0] == 1:
+            g.update_tree_del(algo, e, directed)
+        assert g.checksum() == int(ref[k]), f"step {k}"
+    check_tree(g, og)
+
+
+# -------------------------------------------------------- incremental, batch
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("batch", [1, 64, 4096])
+def test_batches_vs_oracle(algo, batch):
+    scale = 14
+    pairs = gen.rmat(scale, seed=21)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    nb = max(1, min(12, (len(pairs) - imported) // batch))
+    g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs), inc_mode=True)
+    og = oracle_graph(algo, V, pairs[:imported], inc_mode=True)
+    g.build_tree(algo, 0)
+    og.build_tree(0)
+    ref = og.run_batch(pairs, imported, batch, nb, 0)
+    directed = algo != "wcc"
+    for k in range(nb):
+        lo = imported + k * batch
+        hi = min(lo + batch, len(pairs))
+        g.apply_add_pairs(algo, pairs[lo:hi], directed)
+        g.apply_del_pairs(algo, pairs[lo - imported:hi - imported], directed)
+        assert g.checksum() == int(ref[k]), f"batch {k}"
+    val = check_tree(g, og)
+    np.testing.assert_array_equal(val, og.labels()[0])
+
+
+# ------------------------------------------------------------ classification
+@pytest.mark.parametrize("algo", ALGOS)
+def test_classify_matches_tree_semantics(algo):
+    """need_update_tree_add is a pure function of values (bit-exact vs oracle);
+    need_update_tree_del is checked against the GPU's own parents."""
+    scale = 12
+    pairs = gen.rmat(scale, seed=4)
+    V = 1 << scale
+    g = gpu_graph(algo, V, pairs[:50000])
+    og = oracle_graph(algo, V, pairs[:50000])
+    g.build_tree(algo, 0)
+    og.build_tree(0)
+    directed = algo != "wcc"
+    cand = edges_of(algo, pairs[50000:52000])
+    unsafe = g.classify(algo, cand, None, directed)
+    exp = np.array([og.need_update_tree_add(int(e["src"]), int(e["dst"]), int(e["data"])) for e in cand])
+    np.testing.assert_array_equal(unsafe.astype(bool), exp)
+    # deletes: unsafe iff the edge is dst's parent edge (either way if undirected)
+    old = edges_of(algo, pairs[:2000])
+    unsafe = g.classify(algo, old, np.ones(len(old), np.uint8), directed).astype(bool)
+    val, par, pw = g.labels()
+    exp = (par[old["dst"].astype(np.int64)] == old["src"]) & (pw[old["dst"].astype(np.int64)] == old["data"])
+    if not directed:
+        exp |= (par[old["src"].astype(np.int64)] == old["dst"]) & (pw[old["src"].astype(np.int64)] == old["data"])
+    np.testing.assert_array_equal(unsafe, exp)
+
+
+# -------------------------------------------------------------- adjacency
+@pytest.mark.parametrize("weighted,symmetric", [(False, False), (True, False), (False, True)])
+def test_multiplicity_and_degrees(weighted, symmetric):
+    """Old multiplicities, get_edge_num and degrees (IndexedEdgeStorage,
+    core/storage.hpp:345-423) with heavy duplication inside one batch.  Inside
+    a batch the reference's order is a thread race, so the multiset of old
+    counts per (unordered, if undirected) key is compared."""
+    V = 512
+    rng = np.random.default_rng(3)
+    e = np.zeros(3000, rg.EDGE_DTYPE)
+    e["src"] = rng.integers(0, 64, 3000)
+    e["dst"] = rng.integers(0, 64, 3000)
+    e["data"] = rng.integers(1, 4, 3000) if weighted else 0
+    algo = "sssp" if weighted else ("wcc" if symmetric else "bfs")
+    directed = not symmetric
+    g = rg.Graph(V, 4096, symmetric=symmetric, weighted=weighted)
+    og = oracle_graph(algo, V, np.zeros((0, 2), np.uint64))
+
+    def key(arr, old):
+        s, d = arr["src"].tolist(), arr["dst"].tolist()
+        if symmetric:
+            s, d = [min(a, b) for a, b in zip(s, d)], [max(a, b) for a, b in zip(s, d)]
+        return sorted(zip(s, d, arr["data"].tolist(), old.tolist()))
+
+    old = g.add_edges(e, directed)
+    exp = np.array([og.add_edge(int(x["src"]), int(x["dst"]), int(x["data"])) for x in e], np.uint64)
+    assert key(e, old) == key(e, exp)
+    d = e[:1500]
+    old = g.del_edges(d, directed)
+    exp = np.array([og.del_edge(int(x["src"]), int(x["dst"]), int(x["data"])) for x in d], np.uint64)
+    assert key(d, old) == key(d, exp)
+    absent = np.zeros(3, rg.EDGE_DTYPE)
+    absent["src"] = [500, 501, 502]
+    absent["dst"] = [7, 8, 9]
+    assert (g.del_edges(absent, directed) == 0).all()
+    q = e[:500]
+    num = g.get_edge_num(q)
+    exp = np.array([og.get_edge_num(int(x["src"]), int(x["dst"]), int(x["data"])) for x in q])
+    np.testing.assert_array_equal(num, exp)
+    od, idg = g.degrees()
+    np.testing.assert_array_equal(od, [og.out_degree(v) for v in range(V)])
+    np.testing.assert_array_equal(idg, [og.in_degree(v) for v in range(V)])
+
+
+def test_undirected_old_num_conventions():
+    """add_edge(e,false) returns the other orientation's old count, minus one
+    for a self-loop (core/graph.hpp:206-211); del_edge(e,false) the second
+    call's (:232-237)."""
+    og = oracle_graph("wcc", 16, np.zeros((0, 2), np.uint64))
+    g = rg.Graph(16, 64, symmetric=True)
+    seq = [(3, 3), (3, 3), (1, 2), (2, 1), (1, 2), (4, 4)]
+    for s, d in seq:
+        assert g.add_edge(s, d, directed=False) == og.add_edge(s, d)
+    for s, d in seq[::-1] + [(5, 6), (3, 3), (3, 3)]:
+        assert g.del_edge(s, d, directed=False) == og.del_edge(s, d)
+
+
+# --------------------------------------------------------------- edge cases
+def test_errors_are_status_codes():
+    g = rg.Graph(100, 1000, weighted=True)
+    with pytest.raises(rg.RGError) as ei:
+        g.add_edge(5, 100, 3)
+    assert ei.value.status == 2
+    with pytest.raises(rg.RGError) as ei:
+        g.add_edge(5, 6, 1 << 31)
+    assert ei.value.status == 3
+    with pytest.raises(rg.RGError) as ei:
+        g.update_tree_add("sssp", [(1, 2, 3)])
+    assert ei.value.status == 8   # no labels built yet
+    with pytest.raises(rg.RGError):
+        g.build_tree("sssp", 1000)
+    g.build_tree("sssp", 0)
+    # empty batches are no-ops
+    assert len(g.add_edges(np.zeros(0, rg.EDGE_DTYPE))) == 0
+    assert g.update_tree_add("sssp", np.zeros(0, rg.EDGE_DTYPE)) == 0
+    assert g.update_tree_del("sssp", np.zeros(0, rg.EDGE_DTYPE)) == 0
+    g.apply_add("sssp", np.zeros(0, rg.EDGE_DTYPE))
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_empty_graph_and_isolated_root(algo):
+    V = 64
+    g = rg.Graph(V, 128, symmetric=algo == "wcc", weighted=WEIGHTED[algo])
+    g.build_tree(algo, 5)
+    og = oracle_graph(algo, V, np.zeros((0, 2), np.uint64))
+    og.build_tree(5)
+    np.testing.assert_array_equal(g.values(), og.labels()[0])
+    # first edge ever, then its removal
+    e = edges_of(algo, np.array([[5, 9]], np.uint64))
+    g.apply_add(algo, e, algo != "wcc")
+    og.add_edge(5, 9, int(e["data"][0]))
+    og.update_tree_add(5, 9, int(e["data"][0]), 5)
+    np.testing.assert_array_equal(g.values(), og.labels()[0])
+    g.apply_del(algo, e, algo != "wcc")
+    og.del_edge(5, 9, int(e["data"][0]))
+    og.update_tree_del(5, 9, int(e["data"][0]), 5)
+    np.testing.assert_array_equal(g.values(), og.labels()[0])
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_insert_then_delete_restores_values(algo):
+    """Size-independent property: a batch inserted and then deleted leaves the
+    values exactly where they were."""
+    scale = 16
+    pairs = gen.rmat(scale, seed=2)
+    V = 1 << scale
+    base, extra = pairs[:800000], pairs[800000:900000]
+    g = gpu_graph(algo, V, base, hint=len(pairs))
+    g.build_tree(algo, 0)
+    before = g.values()
+    d = algo != "wcc"
+    old = g.apply_add_pairs(algo, extra, d, want_old=True)
+    mid = g.values()
+    g.build_tree(algo, 0)
+    np.testing.assert_array_equal(g.values(), mid)   # incremental == from scratch
+    g.apply_del_pairs(algo, extra, d)
+    np.testing.assert_array_equal(g.values(), before)
+    assert old is not None
+
+
+def test_trace_modified_lists_changed_vertices():
+    pairs = gen.rmat(12, seed=8)
+    V = 4096
+    g = gpu_graph("sssp", V, pairs[:60000], trace=True)
+    g.build_tree("sssp", 0)
+    before = g.values()
+    g.clear_modified()
+    g.apply_add_pairs("sssp", pairs[60000:60100])
+    after = g.values()
+    mod = set(g.get_modified().tolist())
+    changed = set(np.nonzero(before != after)[0].tolist())
+    assert changed <= mod
