@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <cstring>
 
+#include <cub/device/device_scan.cuh>
+
 #include "rg_internal.cuh"
 
 namespace rg {
@@ -144,17 +146,20 @@ __global__ void k_grow(DevDir dir, unsigned long long *ctl, int which) {
     uint32_t v = dir.grow[k];
     if (threadIdx.x == 0) {
       uint32_t len = dir.len[v], cap = dir.cap[v];
-      uint64_t want = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
-      while (want < len) want *= 2;
-      if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
-      unsigned long long off = atomicAdd(dir.pool_top, (unsigned long long)want);
-      if (off + want > dir.pool_cap) {
-        atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
-        s_new_cap = 0;
-      } else {
-        s_new_cap = (uint32_t)want;
+      s_new_cap = 0;
+      if (len > cap) {  // (a retry after compaction skips vertices already grown)
+        uint64_t want = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
+        while (want < len) want *= 2;
+        if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
+        unsigned long long off = atomicAdd(dir.pool_top, (unsigned long long)want);
+        if (off + want > dir.pool_cap) {
+          atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
+          ctl[C_AUX] = 1;  // pool exhausted: the host compacts and retries
+        } else {
+          s_new_cap = (uint32_t)want;
+          s_new_off = off;
+        }
       }
-      s_new_off = off;
       s_copy = len < cap ? len : cap;
     }
     __syncthreads();
@@ -168,6 +173,33 @@ __global__ void k_grow(DevDir dir, unsigned long long *ctl, int which) {
       }
     }
     __syncthreads();
+  }
+}
+
+// Pool compaction: segments keep their capacity and slot order, but are
+// packed back to back into a fresh pool (regions abandoned by growth are
+// reclaimed).  Slot positions inside a segment do not change, so edge records
+// stay valid.
+__global__ void k_caps_u64(const uint32_t *cap, uint64_t V, uint64_t *out) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += stride) out[v] = cap[v];
+}
+
+template <bool W>
+__global__ void k_compact(DevDir dir, const void *old_pool, void *new_pool, const uint64_t *new_off, uint64_t V) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  const E *src = reinterpret_cast<const E *>(old_pool);
+  E *dst = reinterpret_cast<E *>(new_pool);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = warp; v < V; v += nwarps) {
+    uint32_t len = dir.len[v], cap = dir.cap[v];
+    uint32_t n = len < cap ? len : cap;
+    uint64_t from = dir.off[v], to = new_off[v];
+    for (uint32_t i = lane; i < n; i += 32) dst[to + i] = src[from + i];
+    __syncwarp();
+    if (lane == 0) dir.off[v] = to;
   }
 }
 
@@ -348,7 +380,8 @@ int finish(Graph &g, bool need_old, uint64_t *old_num, uint64_t n) {
   RG_CUDA(cudaStreamSynchronize(g.stream));
   if (g.h_ctl[C_ERR]) {
     int code = (int)g.h_ctl[C_ERR];
-    set_error(code == RG_ENOSPACE ? "device edge pool or edge index is full" : "device error");
+    set_error(code == RG_ENOSPACE ? (g.h_ctl[C_AUX] == 1 ? "device edge pool is full" : "device edge index is full")
+                                  : "device error");
     cudaMemsetAsync(&g.d.ctl[C_ERR], 0, 8, g.stream);
     return code;
   }
@@ -374,7 +407,7 @@ int storage_alloc(Graph &g) {
   if (keys < 1024) keys = 1024;
   uint64_t ht_cap = next_pow2(keys + keys / 2);  // load <= 2/3 at the hint
   uint64_t rec_cap = ht_cap - ht_cap / 8;
-  uint64_t pool_cap = keys + keys / 2 + 8 * V + 1024;  // slack for growth
+  uint64_t pool_cap = 2 * keys + 8 * V + 1024;  // slack for growth; compaction reclaims the rest
   size_t esz = g.weighted ? 8 : 4;
   auto alloc = [&](void **p, size_t bytes, const char *what) -> int {
     cudaError_t e = cudaMalloc(p, bytes);
@@ -463,6 +496,72 @@ static int grow_dir(Graph &g, DevDir &dir, int which) {
   return RG_OK;
 }
 
+// Pack one direction's segments into a fresh pool (see k_compact).
+static int compact_dir(Graph &g, DevDir &dir) {
+  const uint64_t V = g.V;
+  uint64_t *offs = nullptr;
+  void *tmp = nullptr, *fresh = nullptr;
+  size_t tmp_bytes = 0;
+  const size_t esz = g.weighted ? 8 : 4;
+  int rc = RG_OK;
+  count_launch(g);
+  k_caps_u64<<<g.num_sms * 8, TPB, 0, g.stream>>>(dir.cap, V, g.scratch64);
+  RG_CUDA(cudaMemsetAsync(g.scratch64 + V, 0, 8, g.stream));
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, g.scratch64, g.scratch64, V + 1, g.stream);
+  cudaError_t e = cudaMalloc(&tmp, tmp_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&offs, (V + 1) * 8);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(tmp);
+    set_error("device allocation failed: pool compaction");
+    return RG_ENOMEM_HBM;
+  }
+  cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, g.scratch64, offs, V + 1, g.stream);
+  uint64_t total = 0;
+  RG_CUDA(cudaMemcpyAsync(&total, offs + V, 8, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  if (total > dir.pool_cap) {
+    set_error("device edge pool is full even after compaction");
+    rc = RG_ENOSPACE;
+  } else if ((e = cudaMalloc(&fresh, dir.pool_cap * esz)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("device allocation failed: pool compaction");
+    rc = RG_ENOMEM_HBM;
+  } else {
+    count_launch(g);
+    if (g.weighted) k_compact<true><<<g.num_sms * 16, TPB, 0, g.stream>>>(dir, dir.pool, fresh, offs, V);
+    else k_compact<false><<<g.num_sms * 16, TPB, 0, g.stream>>>(dir, dir.pool, fresh, offs, V);
+    unsigned long long top = total;
+    cudaMemcpyAsync(dir.pool_top, &top, 8, cudaMemcpyHostToDevice, g.stream);
+    e = cudaStreamSynchronize(g.stream);
+    if (e != cudaSuccess) rc = cuda_fail(e, "pool compaction");
+    cudaFree(dir.pool);
+    dir.pool = fresh;
+  }
+  cudaFree(tmp);
+  cudaFree(offs);
+  if (g.symmetric) g.d.in = g.d.out;
+  return rc;
+}
+
+// Grow the segments that overflowed; if the pool runs out, compact it and
+// grow the rest.
+static int grow_all(Graph &g) {
+  int rc = grow_dir(g, g.d.out, C_GROWN_OUT);
+  if (!rc && !g.symmetric) rc = grow_dir(g, g.d.in, C_GROWN_IN);
+  if (rc) return rc;
+  RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  if (g.h_ctl[C_ERR] != RG_ENOSPACE || g.h_ctl[C_AUX] != 1) return RG_OK;
+  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_ERR], 0, 8, g.stream));
+  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_AUX], 0, 8, g.stream));
+  if ((rc = compact_dir(g, g.d.out))) return rc;
+  if (!g.symmetric && (rc = compact_dir(g, g.d.in))) return rc;
+  rc = grow_dir(g, g.d.out, C_GROWN_OUT);
+  if (!rc && !g.symmetric) rc = grow_dir(g, g.d.in, C_GROWN_IN);
+  return rc;
+}
+
 int storage_add(Graph &g, uint64_t n, uint64_t nops, int directed, uint64_t *old_num, bool collect) {
   OpView ops = op_view(g);
   RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_GROWN_OUT], 0, 16, g.stream));
@@ -471,9 +570,8 @@ int storage_add(Graph &g, uint64_t n, uint64_t nops, int directed, uint64_t *old
     count_launch(g, 4);
     k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
     RG_CUDA(cudaGetLastError());
-    int rc = grow_dir(g, g.d.out, C_GROWN_OUT);
+    int rc = grow_all(g);
     if (rc) return rc;
-    if (!g.symmetric && (rc = grow_dir(g, g.d.in, C_GROWN_IN))) return rc;
     if (g.weighted) {
       k_write_new<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
       k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);

@@ -66,6 +66,8 @@ def test_golden_reference_fixtures(name):
             b = m["batch"]
             for k in range(m["nbatches"]):
                 lo = imported + k * b
+                if lo >= len(pairs):
+                    break
                 hi = min(lo + b, len(pairs))
                 g.apply_add_pairs(algo, pairs[lo:hi], directed)
                 g.apply_del_pairs(algo, pairs[lo - imported:hi - imported], directed)
@@ -308,3 +310,27 @@ def test_trace_modified_lists_changed_vertices():
     mod = set(g.get_modified().tolist())
     changed = set(np.nonzero(before != after)[0].tolist())
     assert changed <= mod
+
+
+def test_pool_compaction_under_churn():
+    """Many small insert batches make segments grow repeatedly; the abandoned
+    regions exhaust the pool and it must be compacted in place of failing."""
+    pairs = gen.rmat(12, seed=13)
+    V = 4096
+    g = rg.Graph(V, len(pairs), weighted=True)
+    for lo in range(0, len(pairs), 1024):
+        g.add_pairs(pairs[lo:lo + 1024], want_old=False)
+    og = oracle_graph("sssp", V, pairs)
+    g.build_tree("sssp", 0)
+    og.build_tree(0)
+    np.testing.assert_array_equal(g.values(), og.labels()[0])
+    check_tree(g, og)
+
+
+def test_pool_exhaustion_is_a_status():
+    """A hint far below the real edge count ends in RG_ENOSPACE, not a fault."""
+    pairs = gen.rmat(12, seed=13)
+    g = rg.Graph(4096, 1000, weighted=True)
+    with pytest.raises(rg.RGError) as ei:
+        g.add_pairs(pairs, want_old=False)
+    assert ei.value.status == 5
