@@ -144,6 +144,15 @@ int rg_launch_count(rg_graph *g, uint64_t *launches);
 int rg_profile(rg_graph *g, int enable);
 int rg_profile_read(rg_graph *g, uint64_t *launches, double *ms);
 
+/* Frontier size entering each push level of the last tree call (up to cap
+ * entries), the number of levels, and the edge slots those levels scanned.
+ * The reference prints the same per-level counts through
+ * continue_reduce_print_func (src/sssp.cpp:71-75). */
+int rg_level_trace(rg_graph *g, uint64_t *sizes, uint64_t cap, uint64_t *levels, uint64_t *edges_scanned);
+/* Device time (ms, CUDA events) of each push level of the last tree call,
+ * recorded only while rg_profile is on. */
+int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
+
 /* Device bytes held by the graph. */
 int rg_device_bytes(rg_graph *g, uint64_t *bytes);
 

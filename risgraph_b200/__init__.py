@@ -69,6 +69,8 @@ def _declare(L):
         "rg_launch_count": [P, P],
         "rg_profile": [P, _int],
         "rg_profile_read": [P, P, P],
+        "rg_level_trace": [P, P, _u64, P, P],
+        "rg_level_times": [P, P, _u64, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -324,6 +326,23 @@ class Graph:
         ms = np.zeros(1, np.float64)
         _check(lib().rg_profile_read(self._h, _p(n), _p(ms)), "rg_profile_read")
         return int(n[0]), float(ms[0])
+
+    def level_trace(self):
+        """(frontier sizes per push level, edge slots scanned) of the last tree call."""
+        n = np.zeros(1, np.uint64)
+        e = np.zeros(1, np.uint64)
+        _check(lib().rg_level_trace(self._h, None, 0, _p(n), _p(e)), "rg_level_trace")
+        sizes = np.zeros(int(n[0]), np.uint64)
+        _check(lib().rg_level_trace(self._h, _p(sizes), len(sizes), _p(n), _p(e)), "rg_level_trace")
+        return sizes, int(e[0])
+
+    def level_times(self):
+        """Per push level device ms of the last tree call (profile() must be on)."""
+        n = np.zeros(1, np.uint64)
+        _check(lib().rg_level_times(self._h, None, 0, _p(n)), "rg_level_times")
+        ms = np.zeros(int(n[0]), np.float64)
+        _check(lib().rg_level_times(self._h, _p(ms), len(ms), _p(n)), "rg_level_times")
+        return ms
 
     def device_bytes(self) -> int:
         b = np.zeros(1, np.uint64)

@@ -188,6 +188,7 @@ int rg_destroy(rg_graph *gh) {
   rg::storage_free(g);
   cudaFree(g.d.lab); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
+  cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp);
   if (g.h_ctl) cudaFreeHost(g.h_ctl);
   if (g.pev[0]) cudaEventDestroy(g.pev[0]);
   if (g.pev[1]) cudaEventDestroy(g.pev[1]);
@@ -396,6 +397,28 @@ int rg_profile_read(rg_graph *gh, uint64_t *launches, double *ms) {
   if (ms) *ms = gh->g.prof_ms;
   gh->g.prof_launches = 0;
   gh->g.prof_ms = 0.0;
+  return RG_OK;
+}
+
+int rg_level_trace(rg_graph *gh, uint64_t *sizes, uint64_t cap, uint64_t *levels, uint64_t *edges_scanned) {
+  int rc = check_graph(gh);
+  if (rc) return rc;
+  Graph &g = gh->g;
+  if (levels) *levels = g.st_frontier.size();
+  for (uint64_t i = 0; sizes && i < cap && i < g.st_frontier.size(); i++) sizes[i] = g.st_frontier[i];
+  if (edges_scanned) {
+    RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * rg::C_COUNT, cudaMemcpyDeviceToHost, g.stream));
+    RG_CUDA(cudaStreamSynchronize(g.stream));
+    *edges_scanned = g.h_ctl[rg::C_EDGES];
+  }
+  return RG_OK;
+}
+
+int rg_level_times(rg_graph *gh, double *ms, uint64_t cap, uint64_t *levels) {
+  if (!gh) return RG_EINVAL;
+  Graph &g = gh->g;
+  if (levels) *levels = g.st_level_ms.size();
+  for (uint64_t i = 0; ms && i < cap && i < g.st_level_ms.size(); i++) ms[i] = g.st_level_ms[i];
   return RG_OK;
 }
 

@@ -23,6 +23,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "risgraph_b200.h"
 
@@ -51,6 +52,7 @@ enum Ctl : int {
   C_MODN = 10,     // modified list length
   C_CHECKSUM = 11,
   C_AUX = 12,
+  C_EDGES = 13,    // edge slots scanned by push levels (work counter)
   C_COUNT = 16
 };
 
@@ -192,9 +194,15 @@ struct Graph {
   uint32_t stamp_epoch = 0;
   uint32_t inv_epoch = 0;
   uint32_t mod_epoch = 1;
-  uint64_t *scratch64 = nullptr;  // V u64 (unpack labels, checksums)
+  uint64_t *scratch64 = nullptr;  // V+1 u64 (unpack labels, frontier degrees, compaction)
+  uint64_t *lb_P = nullptr;       // V+1 u64 frontier degree prefix
+  uint32_t *lb_tile = nullptr;    // tile partition of the edge range
+  void *cub_tmp = nullptr;
+  size_t cub_tmp_bytes = 0;
   // stats of the last tree call
   uint64_t st_levels = 0, st_invalidated = 0, st_recomputes = 0;
+  std::vector<uint64_t> st_frontier;  // frontier size entering each push level
+  std::vector<double> st_level_ms;    // device time of each push level (profiling on)
   uint64_t bytes = 0;
   std::string err;
   cudaStream_t own_stream = nullptr;

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <type_traits>
 
+#include <cub/device/device_scan.cuh>
+
 #include "rg_internal.cuh"
 
 namespace rg {
@@ -30,6 +32,7 @@ namespace {
 constexpr int TPB = 256;
 constexpr uint32_t HUB = 4096;
 constexpr uint32_t CHUNK = 2048;
+constexpr uint64_t LBS_MIN_FRONTIER = 2048;  // smaller frontiers use k_push
 
 template <bool W>
 struct PoolT;
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
   const int lane = lane_id();
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long local = 0;
+  unsigned long long local = 0, scanned = 0;
   for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
     uint64_t i = base + lane;
     uint32_t u = 0, len = 0;
@@ -112,6 +115,7 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
       if (lane >= o) incl += t;
     }
     const uint32_t total = __shfl_sync(FULL, incl, 31);
+    if (lane == 0) scanned += total;
     for (uint32_t kb = 0; kb < total; kb += 32) {
       const uint32_t k = kb + lane;
       const bool valid = k < total;
@@ -141,6 +145,7 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
       if (mst) mark_modified(g, upd, v, mst);
     }
   }
+  if (lane == 0 && scanned) atomicAdd(&g.ctl[C_EDGES], scanned);
   warp_add_result(local, &g.ctl[C_RESULT]);
 }
 
@@ -155,7 +160,7 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
   const int lane = lane_id();
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long local = 0;
+  unsigned long long local = 0, scanned = 0;
   for (uint64_t t = warp; t < n; t += nwarps) {
     const uint64_t task = hubq[t];
     const uint32_t u = (uint32_t)task, c = (uint32_t)(task >> 32);
@@ -163,6 +168,7 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
     const uint64_t off = g.out.off[u];
     const uint64_t su = ld_val(&g.lab[u]);
     const uint32_t start = c * CHUNK, end = min(len, start + CHUNK);
+    if (lane == 0 && end > start) scanned += end - start;
     for (uint32_t kb = start; kb < end; kb += 32) {
       const uint32_t k = kb + lane;
       bool upd = false;
@@ -181,7 +187,146 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
       if (mst) mark_modified(g, upd, v, mst);
     }
   }
+  if (lane == 0 && scanned) atomicAdd(&g.ctl[C_EDGES], scanned);
   warp_add_result(local, &g.ctl[C_RESULT]);
+}
+
+// ---- edge-balanced push for large frontiers -------------------------------
+// The frontier's degrees are prefix-summed (P), the concatenated edge range
+// [0, P[n]) is cut into LB_TILE-edge tiles, and each CTA takes whole tiles:
+// the frontier entries a tile touches are staged in shared memory, and each
+// thread relaxes LB_ITEMS edges strided by the block size (coalesced pool
+// reads).  The edge loads of a thread are all issued before the label loads,
+// and those before any CAS, so each thread keeps LB_ITEMS independent memory
+// round trips in flight instead of one.
+constexpr int LB_TPB = 256;
+constexpr int LB_ITEMS = 8;
+constexpr uint32_t LB_TILE = LB_TPB * LB_ITEMS;
+constexpr uint32_t LB_CAP = 1025;  // staged entries per tile (sparser tiles search P in global memory)
+
+__global__ void k_gather_deg(DevGraph g, const uint32_t *fin, uint64_t n, uint64_t *deg) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += stride)
+    deg[i] = i < n ? seg_len(g.out, fin[i]) : 0;
+}
+
+// tile_lo[t] = last frontier index whose edge range starts at or before t*LB_TILE.
+__global__ void k_partition(const uint64_t *P, uint64_t n, uint32_t *tile_lo) {
+  const uint64_t T = P[n];
+  const uint64_t ntiles = (T + LB_TILE - 1) / LB_TILE;
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles; t += stride) {
+    uint64_t x = t < ntiles ? t * LB_TILE : T;
+    uint64_t lo = 0, hi = n;  // largest i in [0, n] with P[i] <= x
+    while (lo < hi) {
+      uint64_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(&P[mid]) <= x) lo = mid;
+      else hi = mid - 1;
+    }
+    tile_lo[t] = (uint32_t)(lo < n ? lo : (n ? n - 1 : 0));
+  }
+}
+
+template <int A, bool W>
+__global__ void __launch_bounds__(LB_TPB) k_push_lbs(DevGraph g, const uint32_t *fin, uint64_t n, const uint64_t *P,
+                                                     const uint32_t *tile_lo, uint32_t *fout,
+                                                     unsigned long long *fout_n, uint32_t st, uint32_t mst) {
+  using P_ = PoolT<W>;
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.out.pool);
+  __shared__ uint32_t s_rel[LB_CAP];
+  __shared__ uint32_t s_u[LB_CAP];
+  __shared__ uint64_t s_base[LB_CAP];
+  __shared__ uint64_t s_su[LB_CAP];
+  const uint64_t T = P[n];
+  const uint64_t ntiles = (T + LB_TILE - 1) / LB_TILE;
+  unsigned long long local = 0;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t t0 = t * LB_TILE;
+    const uint64_t t1 = min(t0 + LB_TILE, T);
+    const uint32_t lo = tile_lo[t];
+    const uint32_t hi = tile_lo[t + 1];
+    const uint32_t m = hi - lo + 1;
+    const bool staged = m <= LB_CAP;
+    if (staged) {
+      for (uint32_t j = threadIdx.x; j < m; j += LB_TPB) {
+        uint64_t pj = P[lo + j];
+        uint32_t u = fin[lo + j];
+        s_rel[j] = pj <= t0 ? 0u : (uint32_t)(pj - t0);
+        s_u[j] = u;
+        s_base[j] = g.out.off[u] - pj;
+        s_su[j] = ld_val(&g.lab[u]);
+      }
+    }
+    __syncthreads();
+    uint64_t slot[LB_ITEMS], su[LB_ITEMS];
+    uint32_t uu[LB_ITEMS];
+#pragma unroll
+    for (int k = 0; k < LB_ITEMS; k++) {
+      const uint64_t e = t0 + (uint64_t)k * LB_TPB + threadIdx.x;
+      slot[k] = ~0ull;
+      if (e < t1) {
+        uint32_t j;
+        if (staged) {
+          const uint32_t er = (uint32_t)(e - t0);
+          uint32_t a = 0, b = m - 1;  // largest j with s_rel[j] <= er
+          while (a < b) {
+            uint32_t mid = (a + b + 1) >> 1;
+            if (s_rel[mid] <= er) a = mid;
+            else b = mid - 1;
+          }
+          j = a;
+          slot[k] = s_base[j] + e;
+          uu[k] = s_u[j];
+          su[k] = s_su[j];
+        } else {
+          uint64_t a = lo, b = hi;  // many empty entries: search P directly
+          while (a < b) {
+            uint64_t mid = (a + b + 1) >> 1;
+            if (P[mid] <= e) a = mid;
+            else b = mid - 1;
+          }
+          uint32_t u = fin[a];
+          slot[k] = g.out.off[u] + (e - P[a]);
+          uu[k] = u;
+          su[k] = ld_val(&g.lab[u]);
+        }
+      }
+    }
+    typename P_::E ent[LB_ITEMS];
+#pragma unroll
+    for (int k = 0; k < LB_ITEMS; k++)
+      if (slot[k] != ~0ull) ent[k] = __ldg(&pool[slot[k]]);
+    ulonglong2 cur[LB_ITEMS];
+#pragma unroll
+    for (int k = 0; k < LB_ITEMS; k++) {
+      cur[k] = make_ulonglong2(0, 0);
+      if (slot[k] != ~0ull && !(P_::nbr(ent[k]) & DEAD)) cur[k] = ld_lab(&g.lab[P_::nbr(ent[k])]);
+    }
+#pragma unroll
+    for (int k = 0; k < LB_ITEMS; k++) {
+      bool upd = false;
+      uint32_t v = 0;
+      if (slot[k] != ~0ull && !(P_::nbr(ent[k]) & DEAD)) {
+        v = P_::nbr(ent[k]);
+        const uint32_t w = P_::wt(ent[k]);
+        const uint64_t nv = Hook<A>::combine(su[k], w);
+        ulonglong2 c = cur[k];
+        while (Hook<A>::better(nv, c.x)) {
+          ulonglong2 want = make_ulonglong2(nv, pack_parent(uu[k], w));
+          ulonglong2 old = cas128(&g.lab[v], c, want);
+          if (old.x == c.x && old.y == c.y) { upd = true; break; }
+          c = old;
+        }
+      }
+      local += upd;
+      bool app = upd && atomicExch(&g.stamp[v], st) != st;
+      warp_append(app, v, fout, fout_n, FULL);
+      if (mst) mark_modified(g, upd, v, mst);
+    }
+    __syncthreads();
+  }
+  warp_add_result(local, &g.ctl[C_RESULT]);
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&g.ctl[C_EDGES], T);
 }
 
 // build_tree init (core/graph.hpp:886-896): every label to init_label_func,
@@ -494,6 +639,7 @@ int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64
       set_error("push levels did not converge");
       return RG_ETIMEOUT;
     }
+    g.st_frontier.push_back(n);
     int nb = (cur == g.q[0]) ? 1 : 0;
     uint32_t *next = g.q[nb];
     unsigned long long *next_n = &g.d.ctl[C_QN0 + nb];
@@ -501,10 +647,20 @@ int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64
     RG_CUDA(cudaMemsetAsync(hub_n, 0, 8, g.stream));
     uint32_t st = next_stamp(g);
     if (g.profiling) RG_CUDA(cudaEventRecord(g.pev[0], g.stream));
-    count_launch(g, 2);
-    k_push<A, W><<<grid_warps(g, (n + 31) / 32), TPB, 0, g.stream>>>(g.d, cur, cur_n, next, next_n, st, g.hubq, hub_n,
-                                                                      mod_stamp(g));
-    k_push_hub<A, W><<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.hubq, hub_n, next, next_n, st, mod_stamp(g));
+    if (n >= LBS_MIN_FRONTIER) {
+      count_launch(g, 4);
+      k_gather_deg<<<grid_warps(g, (n + 32) / 32), TPB, 0, g.stream>>>(g.d, cur, n, g.scratch64);
+      size_t tb = g.cub_tmp_bytes;
+      RG_CUDA(cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.lb_P, n + 1, g.stream));
+      k_partition<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.lb_P, n, g.lb_tile);
+      k_push_lbs<A, W><<<g.num_sms * 2, LB_TPB, 0, g.stream>>>(g.d, cur, n, g.lb_P, g.lb_tile, next, next_n, st,
+                                                               mod_stamp(g));
+    } else {
+      count_launch(g, 2);
+      k_push<A, W><<<grid_warps(g, (n + 31) / 32), TPB, 0, g.stream>>>(g.d, cur, cur_n, next, next_n, st, g.hubq,
+                                                                        hub_n, mod_stamp(g));
+      k_push_hub<A, W><<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.hubq, hub_n, next, next_n, st, mod_stamp(g));
+    }
     RG_CUDA(cudaGetLastError());
     if (g.profiling) RG_CUDA(cudaEventRecord(g.pev[1], g.stream));
     int rc = read_ctl(g);
@@ -514,6 +670,7 @@ int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64
       RG_CUDA(cudaEventElapsedTime(&ms, g.pev[0], g.pev[1]));
       g.prof_ms += ms;
       g.prof_launches += 1;
+      g.st_level_ms.push_back(ms);
     }
     n = g.h_ctl[C_QN0 + nb];
     cur = next;
@@ -667,6 +824,11 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.scratch64, V * 8 + 8, "scratch"))) return rc;
   g.hubq_cap = g.d.out.pool_cap / CHUNK + V / HUB + 1024;
   if ((rc = alloc((void **)&g.hubq, g.hubq_cap * 8, "hub tasks"))) return rc;
+  if ((rc = alloc((void **)&g.lb_P, V * 8 + 16, "frontier degree prefix"))) return rc;
+  if ((rc = alloc((void **)&g.lb_tile, (g.d.out.pool_cap / LB_TILE + 4) * 4, "tile partition"))) return rc;
+  g.cub_tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, g.cub_tmp_bytes, g.scratch64, g.lb_P, V + 1);
+  if ((rc = alloc(&g.cub_tmp, g.cub_tmp_bytes + 256, "scan scratch"))) return rc;
   if ((rc = alloc((void **)&g.d.ctl, sizeof(unsigned long long) * C_COUNT, "control block"))) return rc;
   RG_CUDA(cudaMemset(g.d.ctl, 0, sizeof(unsigned long long) * C_COUNT));
   RG_CUDA(cudaMemset(g.d.stamp, 0, V * 4 + 4));
@@ -680,6 +842,9 @@ int tree_alloc(Graph &g) {
 
 int tree_build(Graph &g, int algo, uint64_t root, uint64_t *total) {
   g.st_levels = g.st_invalidated = g.st_recomputes = 0;
+  g.st_frontier.clear();
+  g.st_level_ms.clear();
+  cudaMemsetAsync(&g.d.ctl[C_EDGES], 0, 8, g.stream);
   g.algo = algo;
   g.root = root;
   int rc = dispatch(g, algo, 0, root, 1, false);
@@ -690,6 +855,9 @@ int tree_build(Graph &g, int algo, uint64_t root, uint64_t *total) {
 
 int tree_add(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total) {
   g.st_levels = g.st_invalidated = g.st_recomputes = 0;
+  g.st_frontier.clear();
+  g.st_level_ms.clear();
+  cudaMemsetAsync(&g.d.ctl[C_EDGES], 0, 8, g.stream);
   int rc = dispatch(g, g.algo, 1, n_edges, directed, from_cands);
   if (rc) return rc;
   if (total) *total = g.h_ctl[C_RESULT];
@@ -698,6 +866,9 @@ int tree_add(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t
 
 int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total) {
   g.st_levels = g.st_invalidated = g.st_recomputes = 0;
+  g.st_frontier.clear();
+  g.st_level_ms.clear();
+  cudaMemsetAsync(&g.d.ctl[C_EDGES], 0, 8, g.stream);
   int rc = dispatch(g, g.algo, 2, n_edges, directed, from_cands);
   if (rc) return rc;
   if (total) *total = g.h_ctl[C_RESULT];
