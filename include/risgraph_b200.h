@@ -156,6 +156,31 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
 /* Device bytes held by the graph. */
 int rg_device_bytes(rg_graph *g, uint64_t *bytes);
 
+/* Allocation-free build_tree for callers that may not allocate device memory
+ * when they need a tree: a process whose device memory belongs to another
+ * framework's pool and is fixed at start-up, or a latency-critical path where
+ * cudaMalloc/cudaFree would synchronise the device.  No counterpart in the
+ * reference (its build_tree, core/graph.hpp:873-985, works on the Graph's own
+ * storage); this computes the same values with the same hooks.
+ *
+ * Input: a CSR graph in caller-owned DEVICE memory: row_offsets[vertices+1]
+ * (uint64, non-decreasing, last <= edges), columns[edges] (uint32 < vertices),
+ * weights[edges] (uint32, or NULL for unweighted).  Output: values[vertices]
+ * and parents[vertices] (parent == vertices for none) in caller-owned device
+ * memory; either may be NULL, not both.  Runs on cuda_stream (NULL = default)
+ * and returns when done.  No cudaMalloc/cudaFree or allocating library call:
+ * the working memory is one static device array of about 28 MB, reserved on
+ * every GPU that loads the library until exit, which bounds the graph to
+ * RG_STATIC_MAX_VERTICES vertices (larger graphs: RG_EINVAL).  All calls share
+ * that array: calls that overlap on the GPU race and give undefined results.
+ * The first call on each device looks the array's address up (with that device
+ * current); make it before any stream capture.  Malformed CSR input returns
+ * RG_EINVAL / RG_EINVAL_VID without touching memory out of range. */
+#define RG_STATIC_MAX_VERTICES (1u << 20)
+int rg_build_tree_csr_static(int algo, uint64_t root, uint64_t vertices, uint64_t edges,
+                             const uint64_t *row_offsets, const uint32_t *columns, const uint32_t *weights,
+                             uint64_t *values, uint64_t *parents, void *cuda_stream);
+
 const char *rg_status_string(int status);
 /* Last error message of the calling thread ("" if none). */
 const char *rg_last_error(void);

@@ -71,6 +71,7 @@ def _declare(L):
         "rg_profile_read": [P, P, P],
         "rg_level_trace": [P, P, _u64, P, P],
         "rg_level_times": [P, P, _u64, P],
+        "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
