@@ -219,7 +219,7 @@ def main():
     stream = torch.cuda.Stream()
     g.set_stream(stream.cuda_stream)
 
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, 1)):
         g.build_tree(algo, root)
     values = g.values()
     E_r, V_r = reached_edges(pairs, V, values, algo)
