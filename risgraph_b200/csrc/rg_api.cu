@@ -188,7 +188,7 @@ int rg_destroy(rg_graph *gh) {
   rg::storage_free(g);
   cudaFree(g.d.lab); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
-  cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp);
+  cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp); cudaFree(g.act);
   if (g.h_ctl) cudaFreeHost(g.h_ctl);
   if (g.pev[0]) cudaEventDestroy(g.pev[0]);
   if (g.pev[1]) cudaEventDestroy(g.pev[1]);

@@ -65,6 +65,7 @@ struct DevDir {
   uint64_t pool_cap;
   unsigned long long *pool_top;
   uint32_t *grow;   // vertices to grow
+  uint32_t *owner;  // per pool slot: the vertex whose segment holds it (NONE if unused)
 };
 
 struct DevGraph {
@@ -197,6 +198,8 @@ struct Graph {
   uint64_t *scratch64 = nullptr;  // V+1 u64 (unpack labels, frontier degrees, compaction)
   uint64_t *lb_P = nullptr;       // V+1 u64 frontier degree prefix
   uint32_t *lb_tile = nullptr;    // tile partition of the edge range
+  uint32_t *act = nullptr;        // V: level id of the dense level a vertex is active in
+  uint32_t act_epoch = 0;
   void *cub_tmp = nullptr;
   size_t cub_tmp_bytes = 0;
   // stats of the last tree call

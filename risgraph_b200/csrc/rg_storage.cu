@@ -165,7 +165,12 @@ __global__ void k_grow(DevDir dir, unsigned long long *ctl, int which) {
     __syncthreads();
     if (s_new_cap) {
       uint64_t from = dir.off[v];
-      for (uint32_t i = threadIdx.x; i < s_copy; i += blockDim.x) pool[s_new_off + i] = pool[from + i];
+      uint32_t old_cap = dir.cap[v];
+      for (uint32_t i = threadIdx.x; i < s_copy; i += blockDim.x) {
+        pool[s_new_off + i] = pool[from + i];
+        dir.owner[s_new_off + i] = v;
+      }
+      for (uint32_t i = threadIdx.x; i < old_cap; i += blockDim.x) dir.owner[from + i] = NONE;
       __syncthreads();
       if (threadIdx.x == 0) {
         dir.off[v] = s_new_off;
@@ -186,7 +191,8 @@ __global__ void k_caps_u64(const uint32_t *cap, uint64_t V, uint64_t *out) {
 }
 
 template <bool W>
-__global__ void k_compact(DevDir dir, const void *old_pool, void *new_pool, const uint64_t *new_off, uint64_t V) {
+__global__ void k_compact(DevDir dir, const void *old_pool, void *new_pool, uint32_t *new_owner,
+                          const uint64_t *new_off, uint64_t V) {
   using E = typename std::conditional<W, uint2, uint32_t>::type;
   const E *src = reinterpret_cast<const E *>(old_pool);
   E *dst = reinterpret_cast<E *>(new_pool);
@@ -197,7 +203,10 @@ __global__ void k_compact(DevDir dir, const void *old_pool, void *new_pool, cons
     uint32_t len = dir.len[v], cap = dir.cap[v];
     uint32_t n = len < cap ? len : cap;
     uint64_t from = dir.off[v], to = new_off[v];
-    for (uint32_t i = lane; i < n; i += 32) dst[to + i] = src[from + i];
+    for (uint32_t i = lane; i < n; i += 32) {
+      dst[to + i] = src[from + i];
+      new_owner[to + i] = (uint32_t)v;
+    }
     __syncwarp();
     if (lane == 0) dir.off[v] = to;
   }
@@ -216,12 +225,14 @@ __global__ void k_write_new(DevGraph g, OpView ops, uint64_t nops) {
     if (ps < g.out.cap[s]) {
       if constexpr (W) po[g.out.off[s] + ps] = make_uint2(d | DEAD, w);
       else po[g.out.off[s] + ps] = d | DEAD;
+      g.out.owner[g.out.off[s] + ps] = s;
     }
     if (!g.symmetric) {
       uint32_t pd = g.rec_in[rid];
       if (pd < g.in.cap[d]) {
         if constexpr (W) pi[g.in.off[d] + pd] = make_uint2(s | DEAD, w);
         else pi[g.in.off[d] + pd] = s | DEAD;
+        g.in.owner[g.in.off[d] + pd] = d;
       }
     }
   }
@@ -433,6 +444,8 @@ int storage_alloc(Graph &g) {
     if ((rc = alloc((void **)&D.grow, V * 4 + 4, "grow list"))) return rc;
     if ((rc = alloc(&D.pool, pool_cap * esz, "edge pool"))) return rc;
     if ((rc = alloc((void **)&D.pool_top, 8, "pool top"))) return rc;
+    if ((rc = alloc((void **)&D.owner, pool_cap * 4, "slot owners"))) return rc;
+    RG_CUDA(cudaMemset(D.owner, 0xff, pool_cap * 4));
     D.pool_cap = pool_cap;
     RG_CUDA(cudaMemset(D.off, 0, V * 8 + 8));
     RG_CUDA(cudaMemset(D.len, 0, V * 4 + 4));
@@ -458,7 +471,7 @@ void storage_free(Graph &g) {
   for (int dir = 0; dir < (g.symmetric ? 1 : 2); dir++) {
     DevDir &D = dir == 0 ? d.out : d.in;
     cudaFree(D.off); cudaFree(D.len); cudaFree(D.cap); cudaFree(D.deg); cudaFree(D.grow);
-    cudaFree(D.pool); cudaFree(D.pool_top);
+    cudaFree(D.pool); cudaFree(D.pool_top); cudaFree(D.owner);
   }
   cudaFree(d.ht); cudaFree(d.rec_num); cudaFree(d.rec_out); cudaFree(d.rec_in); cudaFree(d.rec_top);
   if (g.ops) cudaFree(g.ops);
@@ -501,6 +514,7 @@ static int compact_dir(Graph &g, DevDir &dir) {
   const uint64_t V = g.V;
   uint64_t *offs = nullptr;
   void *tmp = nullptr, *fresh = nullptr;
+  uint32_t *fresh_owner = nullptr;
   size_t tmp_bytes = 0;
   const size_t esz = g.weighted ? 8 : 4;
   int rc = RG_OK;
@@ -523,20 +537,27 @@ static int compact_dir(Graph &g, DevDir &dir) {
   if (total > dir.pool_cap) {
     set_error("device edge pool is full even after compaction");
     rc = RG_ENOSPACE;
-  } else if ((e = cudaMalloc(&fresh, dir.pool_cap * esz)) != cudaSuccess) {
+  } else if ((e = cudaMalloc(&fresh, dir.pool_cap * esz)) != cudaSuccess ||
+             (e = cudaMalloc(&fresh_owner, dir.pool_cap * 4)) != cudaSuccess) {
     cudaGetLastError();
+    cudaFree(fresh);
     set_error("device allocation failed: pool compaction");
     rc = RG_ENOMEM_HBM;
   } else {
     count_launch(g);
-    if (g.weighted) k_compact<true><<<g.num_sms * 16, TPB, 0, g.stream>>>(dir, dir.pool, fresh, offs, V);
-    else k_compact<false><<<g.num_sms * 16, TPB, 0, g.stream>>>(dir, dir.pool, fresh, offs, V);
+    cudaMemsetAsync(fresh_owner, 0xff, dir.pool_cap * 4, g.stream);
+    if (g.weighted)
+      k_compact<true><<<g.num_sms * 16, TPB, 0, g.stream>>>(dir, dir.pool, fresh, fresh_owner, offs, V);
+    else
+      k_compact<false><<<g.num_sms * 16, TPB, 0, g.stream>>>(dir, dir.pool, fresh, fresh_owner, offs, V);
     unsigned long long top = total;
     cudaMemcpyAsync(dir.pool_top, &top, 8, cudaMemcpyHostToDevice, g.stream);
     e = cudaStreamSynchronize(g.stream);
     if (e != cudaSuccess) rc = cuda_fail(e, "pool compaction");
     cudaFree(dir.pool);
+    cudaFree(dir.owner);
     dir.pool = fresh;
+    dir.owner = fresh_owner;
   }
   cudaFree(tmp);
   cudaFree(offs);

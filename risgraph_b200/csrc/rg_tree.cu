@@ -30,8 +30,8 @@ namespace rg {
 namespace {
 
 constexpr int TPB = 256;
-constexpr uint32_t HUB = 4096;
-constexpr uint32_t CHUNK = 2048;
+constexpr uint32_t HUB = 64;     // longer lists of a small frontier are split into
+constexpr uint32_t CHUNK = 64;   // CHUNK-slot tasks so no warp walks a long list alone
 constexpr uint64_t LBS_MIN_FRONTIER = 2048;  // smaller frontiers use k_push
 
 template <bool W>
@@ -191,6 +191,78 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
   warp_add_result(local, &g.ctl[C_RESULT]);
 }
 
+// Relaxation of N independent candidate edges held by one thread (u[k] -> v[k]
+// with weight w[k], source value su[k], target record cur[k] already loaded).
+// All CASes are issued before any result is used, then all stamp exchanges,
+// then one warp-wide append for every new frontier entry of the warp: the
+// success path costs three round trips per N edges instead of three per edge.
+template <int A, int N>
+__device__ __forceinline__ void relax_batch(const DevGraph &g, const bool (&on)[N], const uint32_t (&u)[N],
+                                            const uint32_t (&v)[N], const uint32_t (&w)[N],
+                                            const uint64_t (&su)[N], ulonglong2 (&cur)[N], uint32_t st,
+                                            uint32_t *fout, unsigned long long *fout_n, unsigned long long &local,
+                                            uint32_t mst) {
+  bool pend[N], upd[N];
+  ulonglong2 want[N], old[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    const uint64_t nv = Hook<A>::combine(su[k], w[k]);
+    pend[k] = on[k] && Hook<A>::better(nv, cur[k].x);
+    want[k] = make_ulonglong2(nv, pack_parent(u[k], w[k]));
+    upd[k] = false;
+  }
+#pragma unroll
+  for (int k = 0; k < N; k++)
+    if (pend[k]) old[k] = cas128(&g.lab[v[k]], cur[k], want[k]);
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    if (!pend[k]) continue;
+    if (old[k].x == cur[k].x && old[k].y == cur[k].y) {
+      upd[k] = true;
+      continue;
+    }
+    cur[k] = old[k];
+    while (Hook<A>::better(want[k].x, cur[k].x)) {  // lost a race: retry while still better
+      ulonglong2 o = cas128(&g.lab[v[k]], cur[k], want[k]);
+      if (o.x == cur[k].x && o.y == cur[k].y) {
+        upd[k] = true;
+        break;
+      }
+      cur[k] = o;
+    }
+  }
+  uint32_t ex[N];
+#pragma unroll
+  for (int k = 0; k < N; k++)
+    if (upd[k]) ex[k] = atomicExch(&g.stamp[v[k]], st);
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    local += upd[k];
+    cnt += (upd[k] && ex[k] != st);
+  }
+  // one atomic per warp for all new entries
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(FULL, incl, o);
+    if (lane_id() >= o) incl += t;
+  }
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  if (total) {
+    unsigned long long base = 0;
+    if (lane_id() == 31) base = atomicAdd(fout_n, (unsigned long long)total);
+    base = __shfl_sync(FULL, base, 31) + (incl - cnt);
+#pragma unroll
+    for (int k = 0; k < N; k++)
+      if (upd[k] && ex[k] != st) fout[base++] = v[k];
+  }
+  if (mst) {
+#pragma unroll
+    for (int k = 0; k < N; k++) mark_modified(g, upd[k], v[k], mst);
+  }
+}
+
 // ---- edge-balanced push for large frontiers -------------------------------
 // The frontier's degrees are prefix-summed (P), the concatenated edge range
 // [0, P[n]) is cut into LB_TILE-edge tiles, and each CTA takes whole tiles:
@@ -200,7 +272,7 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
 // and those before any CAS, so each thread keeps LB_ITEMS independent memory
 // round trips in flight instead of one.
 constexpr int LB_TPB = 256;
-constexpr int LB_ITEMS = 8;
+constexpr int LB_ITEMS = 4;
 constexpr uint32_t LB_TILE = LB_TPB * LB_ITEMS;
 constexpr uint32_t LB_CAP = 1025;  // staged entries per tile (sparser tiles search P in global memory)
 
@@ -228,7 +300,7 @@ __global__ void k_partition(const uint64_t *P, uint64_t n, uint32_t *tile_lo) {
 }
 
 template <int A, bool W>
-__global__ void __launch_bounds__(LB_TPB) k_push_lbs(DevGraph g, const uint32_t *fin, uint64_t n, const uint64_t *P,
+__global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32_t *fin, uint64_t n, const uint64_t *P,
                                                      const uint32_t *tile_lo, uint32_t *fout,
                                                      unsigned long long *fout_n, uint32_t st, uint32_t mst) {
   using P_ = PoolT<W>;
@@ -292,41 +364,129 @@ __global__ void __launch_bounds__(LB_TPB) k_push_lbs(DevGraph g, const uint32_t 
         }
       }
     }
-    typename P_::E ent[LB_ITEMS];
+    bool on[LB_ITEMS];
+    uint32_t vv[LB_ITEMS], ww[LB_ITEMS];
 #pragma unroll
-    for (int k = 0; k < LB_ITEMS; k++)
-      if (slot[k] != ~0ull) ent[k] = __ldg(&pool[slot[k]]);
+    for (int k = 0; k < LB_ITEMS; k++) {
+      on[k] = false;
+      vv[k] = 0;
+      ww[k] = 0;
+      if (slot[k] != ~0ull) {
+        typename P_::E ent = __ldg(&pool[slot[k]]);
+        vv[k] = P_::nbr(ent);
+        ww[k] = P_::wt(ent);
+        on[k] = !(vv[k] & DEAD);
+      } else {
+        uu[k] = 0;
+        su[k] = 0;
+      }
+    }
     ulonglong2 cur[LB_ITEMS];
 #pragma unroll
-    for (int k = 0; k < LB_ITEMS; k++) {
-      cur[k] = make_ulonglong2(0, 0);
-      if (slot[k] != ~0ull && !(P_::nbr(ent[k]) & DEAD)) cur[k] = ld_lab(&g.lab[P_::nbr(ent[k])]);
-    }
-#pragma unroll
-    for (int k = 0; k < LB_ITEMS; k++) {
-      bool upd = false;
-      uint32_t v = 0;
-      if (slot[k] != ~0ull && !(P_::nbr(ent[k]) & DEAD)) {
-        v = P_::nbr(ent[k]);
-        const uint32_t w = P_::wt(ent[k]);
-        const uint64_t nv = Hook<A>::combine(su[k], w);
-        ulonglong2 c = cur[k];
-        while (Hook<A>::better(nv, c.x)) {
-          ulonglong2 want = make_ulonglong2(nv, pack_parent(uu[k], w));
-          ulonglong2 old = cas128(&g.lab[v], c, want);
-          if (old.x == c.x && old.y == c.y) { upd = true; break; }
-          c = old;
-        }
-      }
-      local += upd;
-      bool app = upd && atomicExch(&g.stamp[v], st) != st;
-      warp_append(app, v, fout, fout_n, FULL);
-      if (mst) mark_modified(g, upd, v, mst);
-    }
+    for (int k = 0; k < LB_ITEMS; k++) cur[k] = on[k] ? ld_lab(&g.lab[vv[k]]) : make_ulonglong2(0, 0);
+    relax_batch<A, LB_ITEMS>(g, on, uu, vv, ww, su, cur, st, fout, fout_n, local, mst);
     __syncthreads();
   }
   warp_add_result(local, &g.ctl[C_RESULT]);
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&g.ctl[C_EDGES], T);
+}
+
+// ---- edge-centric push for dense levels -----------------------------------
+// When the frontier holds a large share of the vertices (the reference switches
+// to its dense mode at the same point, core/graph.hpp:334), streaming the whole
+// out-pool beats locating every frontier segment: slot i belongs to owner[i]
+// and is relaxed when its owner is active in this level (act[owner] == id).
+// Reads of owner[] and of the pool are fully coalesced; there is no staging,
+// search or barrier, and each thread keeps DN_ITEMS slots in flight.
+constexpr int DN_TPB = 256;
+constexpr int DN_ITEMS = 4;
+constexpr uint64_t DENSE_DIV = 20;  // dense when frontier >= V / DENSE_DIV
+
+__global__ void k_mark_active(const uint32_t *fin, uint64_t n, uint32_t *act, uint32_t id) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) act[fin[i]] = id;
+}
+
+template <int A, bool W>
+__global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint32_t *act, uint32_t act_id,
+                                                       uint32_t *fout, unsigned long long *fout_n, uint32_t st,
+                                                       uint32_t mst) {
+  using P_ = PoolT<W>;
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.out.pool);
+  const uint64_t top = *g.out.pool_top;
+  const uint64_t slots = top < g.out.pool_cap ? top : g.out.pool_cap;
+  const uint64_t tile = (uint64_t)DN_TPB * DN_ITEMS;
+  unsigned long long local = 0, scanned = 0;
+  for (uint64_t base = blockIdx.x * tile; base < slots; base += (uint64_t)gridDim.x * tile) {
+    uint32_t o[DN_ITEMS];
+#pragma unroll
+    for (int k = 0; k < DN_ITEMS; k++) {
+      const uint64_t i = base + (uint64_t)k * DN_TPB + threadIdx.x;
+      o[k] = i < slots ? __ldg(&g.out.owner[i]) : NONE;
+    }
+    bool a[DN_ITEMS];
+#pragma unroll
+    for (int k = 0; k < DN_ITEMS; k++) a[k] = o[k] != NONE && __ldg(&act[o[k]]) == act_id;
+    uint32_t vv[DN_ITEMS], ww[DN_ITEMS];
+    uint64_t su[DN_ITEMS];
+#pragma unroll
+    for (int k = 0; k < DN_ITEMS; k++) {
+      vv[k] = 0;
+      ww[k] = 0;
+      su[k] = 0;
+      if (a[k]) {
+        typename P_::E ent = __ldg(&pool[base + (uint64_t)k * DN_TPB + threadIdx.x]);
+        su[k] = ld_val(&g.lab[o[k]]);
+        vv[k] = P_::nbr(ent);
+        ww[k] = P_::wt(ent);
+        a[k] = !(vv[k] & DEAD);
+        scanned++;
+      }
+    }
+    ulonglong2 cur[DN_ITEMS];
+#pragma unroll
+    for (int k = 0; k < DN_ITEMS; k++) cur[k] = a[k] ? ld_lab(&g.lab[vv[k]]) : make_ulonglong2(0, 0);
+    relax_batch<A, DN_ITEMS>(g, a, o, vv, ww, su, cur, st, fout, fout_n, local, mst);
+  }
+  warp_add_result(local, &g.ctl[C_RESULT]);
+  warp_add_result(scanned, &g.ctl[C_EDGES]);
+}
+
+// Bottom-up BFS level for full builds (the reference's dense pull,
+// core/graph.hpp:936-976, specialised to BFS): every unreached vertex scans
+// its in-edges and takes the first in-neighbour at depth d as its parent,
+// stopping there.  Used when the frontier is large; each vertex is written
+// only by its own thread, so no atomics on labels.
+template <bool W>
+__global__ void k_bfs_bottom_up(DevGraph g, uint64_t d, uint32_t *fout, unsigned long long *fout_n) {
+  using P_ = PoolT<W>;
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.in.pool);
+  const uint64_t V = g.V;
+  unsigned long long local = 0, scanned = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < V; base += stride) {
+    const uint64_t v = base + threadIdx.x;
+    bool found = false;
+    if (v < V && ld_val(&g.lab[v]) == BFS_MAXL) {
+      const uint32_t len = seg_len(g.in, (uint32_t)v);
+      const uint64_t off = g.in.off[v];
+      for (uint32_t k = 0; k < len; k++) {
+        const typename P_::E e = __ldg(&pool[off + k]);
+        const uint32_t u = P_::nbr(e);
+        scanned++;
+        if (u & DEAD) continue;
+        if (ld_val(&g.lab[u]) == d) {
+          g.lab[v] = make_ulonglong2(d + 1, pack_parent(u, P_::wt(e)));
+          found = true;
+          break;
+        }
+      }
+    }
+    local += found;
+    warp_append(found, (uint32_t)v, fout, fout_n, FULL);
+  }
+  warp_add_result(local, &g.ctl[C_RESULT]);
+  warp_add_result(scanned, &g.ctl[C_EDGES]);
 }
 
 // build_tree init (core/graph.hpp:886-896): every label to init_label_func,
@@ -626,7 +786,7 @@ int read_ctl(Graph &g) {
 // Push levels to a fixpoint from the frontier (fin, *fin_n) with n0 entries
 // (do_update_tree_add, core/graph.hpp:1013-1111; build_tree :898-983).
 template <int A, bool W>
-int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64_t n0) {
+int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64_t n0, bool bfs_levels = false) {
   const uint32_t *cur = fin;
   unsigned long long *cur_n = fin_n;
   uint64_t n = n0;
@@ -647,13 +807,26 @@ int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64
     RG_CUDA(cudaMemsetAsync(hub_n, 0, 8, g.stream));
     uint32_t st = next_stamp(g);
     if (g.profiling) RG_CUDA(cudaEventRecord(g.pev[0], g.stream));
-    if (n >= LBS_MIN_FRONTIER) {
+    if (A == RG_BFS && bfs_levels && n * DENSE_DIV >= g.V) {
+      // full BFS build: the frontier is exactly depth lvl; pull bottom-up
+      count_launch(g);
+      k_bfs_bottom_up<W><<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, lvl, next, next_n);
+    } else if (n * DENSE_DIV >= g.V) {
+      if (++g.act_epoch == 0xFFFFFFFFu) {
+        RG_CUDA(cudaMemsetAsync(g.act, 0, (size_t)g.V * 4, g.stream));
+        g.act_epoch = 1;
+      }
+      count_launch(g, 2);
+      k_mark_active<<<grid_warps(g, (n + 31) / 32), TPB, 0, g.stream>>>(cur, n, g.act, g.act_epoch);
+      k_push_dense<A, W><<<g.num_sms * 3, DN_TPB, 0, g.stream>>>(g.d, g.act, g.act_epoch, next, next_n, st,
+                                                                 mod_stamp(g));
+    } else if (n >= LBS_MIN_FRONTIER) {
       count_launch(g, 4);
       k_gather_deg<<<grid_warps(g, (n + 32) / 32), TPB, 0, g.stream>>>(g.d, cur, n, g.scratch64);
       size_t tb = g.cub_tmp_bytes;
       RG_CUDA(cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.lb_P, n + 1, g.stream));
       k_partition<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.lb_P, n, g.lb_tile);
-      k_push_lbs<A, W><<<g.num_sms * 2, LB_TPB, 0, g.stream>>>(g.d, cur, n, g.lb_P, g.lb_tile, next, next_n, st,
+      k_push_lbs<A, W><<<g.num_sms * 3, LB_TPB, 0, g.stream>>>(g.d, cur, n, g.lb_P, g.lb_tile, next, next_n, st,
                                                                mod_stamp(g));
     } else {
       count_launch(g, 2);
@@ -695,7 +868,7 @@ int build_impl(Graph &g, uint64_t root) {
     // every label is rewritten; the modified list becomes "all vertices" lazily
     // through the same dedup stamps.
   }
-  return push_levels<A, W>(g, g.q[0], &g.d.ctl[C_QN0], n0);
+  return push_levels<A, W>(g, g.q[0], &g.d.ctl[C_QN0], n0, /*bfs_levels=*/true);
 }
 
 template <int A, bool W>
@@ -825,6 +998,8 @@ int tree_alloc(Graph &g) {
   g.hubq_cap = g.d.out.pool_cap / CHUNK + V / HUB + 1024;
   if ((rc = alloc((void **)&g.hubq, g.hubq_cap * 8, "hub tasks"))) return rc;
   if ((rc = alloc((void **)&g.lb_P, V * 8 + 16, "frontier degree prefix"))) return rc;
+  if ((rc = alloc((void **)&g.act, V * 4 + 4, "dense-level activity"))) return rc;
+  RG_CUDA(cudaMemset(g.act, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.lb_tile, (g.d.out.pool_cap / LB_TILE + 4) * 4, "tile partition"))) return rc;
   g.cub_tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, g.cub_tmp_bytes, g.scratch64, g.lb_P, V + 1);
