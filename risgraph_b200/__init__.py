@@ -72,6 +72,8 @@ def _declare(L):
         "rg_level_trace": [P, P, _u64, P, P],
         "rg_level_times": [P, P, _u64, P],
         "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
+        "rg_set_option": [P, _int, _u64],
+        "rg_get_option": [P, _int, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -336,6 +338,16 @@ class Graph:
         sizes = np.zeros(int(n[0]), np.uint64)
         _check(lib().rg_level_trace(self._h, _p(sizes), len(sizes), _p(n), _p(e)), "rg_level_trace")
         return sizes, int(e[0])
+
+    OPTIONS = {"dense_pull": 0, "dense_div": 1, "lbs_min": 2, "bfs_bottom_up": 3, "recompute_min": 4}
+
+    def set_option(self, name: str, value: int):
+        _check(lib().rg_set_option(self._h, self.OPTIONS[name], int(value)), "rg_set_option")
+
+    def get_option(self, name: str) -> int:
+        v = np.zeros(1, np.uint64)
+        _check(lib().rg_get_option(self._h, self.OPTIONS[name], _p(v)), "rg_get_option")
+        return int(v[0])
 
     def level_times(self):
         """Per push level device ms of the last tree call (profile() must be on)."""

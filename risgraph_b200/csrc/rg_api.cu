@@ -81,18 +81,29 @@ int edge_updates(rg_graph *gh, const rg_edge *edges, const uint64_t *pairs, uint
   Graph &g = gh->g;
   int rc = check_edges(g, edges, pairs, n);
   if (rc) return rc;
-  for (uint64_t b = 0; b < n || (n == 0 && b == 0); b += CHUNK_EDGES) {
+  const int what = add ? 1 : 2;
+  for (uint64_t b = 0; b < n; b += CHUNK_EDGES) {
     uint64_t m = std::min(CHUNK_EDGES, n - b), nops = 0;
-    if (n == 0) break;
     rc = rg::stage_edges(g, edges ? edges + b : nullptr, pairs ? pairs + 2 * b : nullptr, m, directed, &nops);
     if (rc) return rc;
-    rc = add ? rg::storage_add(g, m, nops, directed, old_num ? old_num + b : nullptr, apply)
-             : rg::storage_del(g, m, nops, directed, old_num ? old_num + b : nullptr, apply);
+    // storage update, candidate list and tree repair in one submission
+    rc = rg::storage_enqueue(g, add, m, nops, directed, apply);
+    if (!rc && apply) rc = rg::tree_enqueue(g, what, m, directed, true);
+    if (!rc && old_num) rc = rg::storage_copy_old(g, m);
+    if (!rc) rc = rg::sync_ctl(g);
     if (rc) return rc;
-    if (apply && g.h_ctl[rg::C_CANDN]) {
-      rc = add ? rg::tree_add(g, m, directed, true, nullptr) : rg::tree_del(g, m, directed, true, nullptr);
+    if (add && g.h_ctl[rg::C_ERR] == RG_ENOSPACE && g.h_ctl[rg::C_AUX] == 1) {
+      // growth ran out of pool: compact, then replay from the growth step
+      rc = rg::storage_recover(g);
+      if (!rc) rc = rg::storage_replay(g, m, nops, directed, apply);
+      if (!rc && apply) rc = rg::tree_enqueue(g, what, m, directed, true);
+      if (!rc && old_num) rc = rg::storage_copy_old(g, m);
+      if (!rc) rc = rg::sync_ctl(g);
       if (rc) return rc;
     }
+    if ((rc = rg::storage_error(g))) return rc;
+    if (apply && (rc = rg::tree_after_sync(g, what, nullptr))) return rc;
+    if (old_num) std::memcpy(old_num + b, rg::storage_old_host(g), m * 8);
   }
   return RG_OK;
 }
@@ -186,12 +197,19 @@ int rg_destroy(rg_graph *gh) {
   cudaSetDevice(g.device);
   if (g.stream) cudaStreamSynchronize(g.stream);
   rg::storage_free(g);
-  cudaFree(g.d.lab); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
+  cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
   cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp); cudaFree(g.act);
+  cudaFree(g.pull_P); cudaFree(g.pull_base); cudaFree(g.pull_tile); cudaFree(g.lb_sums);
   if (g.h_ctl) cudaFreeHost(g.h_ctl);
   if (g.pev[0]) cudaEventDestroy(g.pev[0]);
   if (g.pev[1]) cudaEventDestroy(g.pev[1]);
+  for (auto &l : g.loops)
+    if (l.exec) cudaGraphExecDestroy(l.exec);
+  for (auto &l : g.dels)
+    if (l.exec) cudaGraphExecDestroy(l.exec);
+  if (g.cap_stream) cudaStreamDestroy(g.cap_stream);
+  cudaFree(g.d.trace);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
   delete gh;
   return RG_OK;
@@ -345,6 +363,8 @@ int rg_clear_modified(rg_graph *gh) {
     g.mod_epoch = 1;
   }
   RG_CUDA(cudaMemsetAsync(&g.d.ctl[rg::C_MODN], 0, 8, g.stream));
+  unsigned long long ep = g.mod_epoch;
+  RG_CUDA(cudaMemcpyAsync(&g.d.ctl[rg::C_MODEPOCH], &ep, 8, cudaMemcpyHostToDevice, g.stream));
   RG_CUDA(cudaStreamSynchronize(g.stream));
   return RG_OK;
 }
@@ -404,12 +424,14 @@ int rg_level_trace(rg_graph *gh, uint64_t *sizes, uint64_t cap, uint64_t *levels
   int rc = check_graph(gh);
   if (rc) return rc;
   Graph &g = gh->g;
-  if (levels) *levels = g.st_frontier.size();
-  for (uint64_t i = 0; sizes && i < cap && i < g.st_frontier.size(); i++) sizes[i] = g.st_frontier[i];
-  if (edges_scanned) {
-    RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * rg::C_COUNT, cudaMemcpyDeviceToHost, g.stream));
-    RG_CUDA(cudaStreamSynchronize(g.stream));
-    *edges_scanned = g.h_ctl[rg::C_EDGES];
+  RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * rg::C_COUNT, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  uint64_t n = std::min<uint64_t>(g.h_ctl[rg::C_LEVEL], rg::TRACE_CAP);
+  if (levels) *levels = n;
+  if (edges_scanned) *edges_scanned = g.h_ctl[rg::C_EDGES];
+  if (sizes && cap && n) {
+    uint64_t k = std::min(cap, n);
+    RG_CUDA(cudaMemcpy(sizes, g.d.trace, k * 8, cudaMemcpyDeviceToHost));
   }
   return RG_OK;
 }
@@ -420,6 +442,34 @@ int rg_level_times(rg_graph *gh, double *ms, uint64_t cap, uint64_t *levels) {
   if (levels) *levels = g.st_level_ms.size();
   for (uint64_t i = 0; ms && i < cap && i < g.st_level_ms.size(); i++) ms[i] = g.st_level_ms[i];
   return RG_OK;
+}
+
+int rg_set_option(rg_graph *gh, int option, uint64_t value) {
+  if (!gh) return RG_EINVAL;
+  Graph &g = gh->g;
+  switch (option) {
+    case RG_OPT_DENSE_PULL: g.dense_pull = value ? 1 : 0; return RG_OK;
+    case RG_OPT_DENSE_DIV: g.dense_div = value ? value : 1; return RG_OK;
+    case RG_OPT_LBS_MIN: g.lbs_min = value; return RG_OK;
+    case RG_OPT_BFS_BOTTOM_UP: g.bfs_bottom_up = value ? 1 : 0; return RG_OK;
+    case RG_OPT_RECOMPUTE_MIN: g.recompute_min = value; return RG_OK;
+  }
+  rg::set_error("unknown option");
+  return RG_EINVAL;
+}
+
+int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
+  if (!gh || !value) return RG_EINVAL;
+  Graph &g = gh->g;
+  switch (option) {
+    case RG_OPT_DENSE_PULL: *value = (uint64_t)g.dense_pull; return RG_OK;
+    case RG_OPT_DENSE_DIV: *value = g.dense_div; return RG_OK;
+    case RG_OPT_LBS_MIN: *value = g.lbs_min; return RG_OK;
+    case RG_OPT_BFS_BOTTOM_UP: *value = (uint64_t)g.bfs_bottom_up; return RG_OK;
+    case RG_OPT_RECOMPUTE_MIN: *value = g.recompute_min; return RG_OK;
+  }
+  rg::set_error("unknown option");
+  return RG_EINVAL;
 }
 
 int rg_device_bytes(rg_graph *gh, uint64_t *bytes) {

@@ -53,8 +53,30 @@ enum Ctl : int {
   C_CHECKSUM = 11,
   C_AUX = 12,
   C_EDGES = 13,    // edge slots scanned by push levels (work counter)
-  C_COUNT = 16
+  // device-driven level loop (written by k_level_begin, read by level kernels)
+  C_LEVEL = 16,    // levels run in the current loop
+  C_STAMP = 17,    // frontier dedup stamp of the current level
+  C_ACT = 18,      // activity id of the current dense push level
+  C_MODE = 19,     // mode of the current level (LevelMode)
+  C_DEPTH = 20,    // BFS depth of the current frontier (full builds)
+  C_MODEPOCH = 21, // modified-list epoch (trace_modified graphs)
+  C_KLAUNCH = 22,  // kernels run by the level-loop graph of the current call
+  C_INVTAG = 23,   // invalidation tag of the current deletion repair (tag+1 = rescued)
+  C_INVITER = 24,  // invalidation levels run by the current deletion repair
+  C_ROOT = 25,     // root of the label set (init_label_func argument)
+  C_COUNT = 32
 };
+
+enum LevelMode : unsigned long long {
+  M_EMPTY = 0,      // frontier empty: every level kernel returns at once
+  M_SPARSE = 1,     // k_push + k_push_hub over the frontier list
+  M_PULL = 2,       // k_pull_dense over all in-edges
+  M_DENSE_PUSH = 3, // k_push_dense over all out-slots of active vertices
+  M_BOTTOM_UP = 4,  // k_bfs_bottom_up (full BFS builds)
+  M_LBS = 5,        // edge-balanced push (degree scan + tile partition + k_push_lbs)
+  M_COUNT = 6
+};
+constexpr int TRACE_CAP = 4096;
 
 struct DevDir {
   uint64_t *off;
@@ -78,11 +100,13 @@ struct DevGraph {
   unsigned long long *rec_top;
   uint64_t rec_cap;
   ulonglong2 *lab;
+  uint32_t *val32;   // 32-bit mirror of lab[].x for reads (equal at kernel boundaries)
   uint32_t *stamp;
   uint32_t *inv;
   uint32_t *modstamp;
   uint32_t *modq;
   unsigned long long *ctl;
+  unsigned long long *trace;  // frontier size per level (TRACE_CAP entries)
 };
 
 // ---- per-algorithm hooks (a8): update_func = better(combine(s,w), d);
@@ -117,6 +141,18 @@ struct Hook<RG_WCC> {  // src/wcc.cpp:62-86
   static __host__ __device__ __forceinline__ uint64_t init(uint64_t v, uint64_t) { return v; }
   static constexpr bool all_active = true;
 };
+
+// Values of all four hook sets stay below 2^31 (BFS <= 65536, SSSP/SSWP <=
+// 2^27, WCC < |V| < 2^31), so a 32-bit mirror holds them exactly.  After a
+// successful CAS of the 16-byte record the mirror moves the same way with a
+// fire-and-forget atomic; readers may see it lag within a kernel (a weaker
+// value only costs a wasted CAS or a later relaxation), never run ahead.
+template <int A>
+__device__ __forceinline__ void mirror_improve(uint32_t *m, uint32_t v, uint64_t nv) {
+  if constexpr (A == RG_SSWP) atomicMax(&m[v], (uint32_t)nv);
+  else atomicMin(&m[v], (uint32_t)nv);
+}
+__device__ __forceinline__ uint64_t ld_v32(const uint32_t *m, uint32_t v) { return __ldcg(&m[v]); }
 
 __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
   uint64_t z = x + 0x9E3779B97F4A7C15ull;
@@ -169,6 +205,13 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t *q, 
   if (pred) q[base + __popc(b & ((1u << lane_id()) - 1))] = v;
 }
 
+// A cached, instantiated level-loop graph.
+struct LoopGraph {
+  cudaGraphExec_t exec = nullptr;
+  uint64_t key = 0;
+  int launches = 0;
+};
+
 // ---- host-side graph object ----
 struct Graph {
   DevGraph d{};
@@ -198,8 +241,21 @@ struct Graph {
   uint64_t *scratch64 = nullptr;  // V+1 u64 (unpack labels, frontier degrees, compaction)
   uint64_t *lb_P = nullptr;       // V+1 u64 frontier degree prefix
   uint32_t *lb_tile = nullptr;    // tile partition of the edge range
+  uint64_t *lb_sums = nullptr;    // per-block sums of the device-side frontier scan
   uint32_t *act = nullptr;        // V: level id of the dense level a vertex is active in
   uint32_t act_epoch = 0;
+  // static in-edge partition for dense pull levels, valid while adj_version == pull_version
+  uint64_t *pull_P = nullptr, *pull_base = nullptr;
+  uint32_t *pull_tile = nullptr;
+  uint64_t adj_version = 1, pull_version = 0;
+  int dense_pull = 1;  // dense levels: 1 = pull over in-edges, 0 = edge-centric push
+  uint64_t dense_div = 20, lbs_min = 2048, recompute_min = 2000000;
+  int bfs_bottom_up = 1;
+  // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
+  LoopGraph loops[16];
+  LoopGraph dels[8];
+  cudaStream_t cap_stream = nullptr;
+  uint64_t layout_version = 1;  // bumped when pool buffers move (compaction)
   void *cub_tmp = nullptr;
   size_t cub_tmp_bytes = 0;
   // stats of the last tree call
@@ -235,8 +291,19 @@ void storage_free(Graph &g);
 // Stage n edges (rg_edge or reference pairs) into the device op arrays as
 // directed ops (2 per edge when undirected).  Returns number of ops.
 int stage_edges(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, uint64_t *nops);
-int storage_add(Graph &g, uint64_t n_edges, uint64_t nops, int directed, uint64_t *old_num, bool collect);
-int storage_del(Graph &g, uint64_t n_edges, uint64_t nops, int directed, uint64_t *old_num, bool collect);
+// One staged batch: storage_enqueue launches the multiplicity update (and, when
+// collect, the tree-repair candidate list) without waiting; after sync_ctl,
+// storage_error reports a device error.  A pool exhausted by growth is
+// recovered by storage_recover + storage_replay.  storage_copy_old enqueues
+// the per-edge old counts into pinned memory, read with storage_old_host
+// after the sync.
+int storage_enqueue(Graph &g, bool add, uint64_t n_edges, uint64_t nops, int directed, bool collect);
+int storage_replay(Graph &g, uint64_t n_edges, uint64_t nops, int directed, bool collect);
+int storage_recover(Graph &g);
+int storage_copy_old(Graph &g, uint64_t n_edges);
+const uint64_t *storage_old_host(Graph &g);
+int storage_error(Graph &g);
+int sync_ctl(Graph &g);
 int storage_num(Graph &g, uint64_t nops, uint64_t *num);
 // op array accessors (device pointers)
 uint32_t *op_src(Graph &g);
@@ -250,6 +317,11 @@ int tree_build(Graph &g, int algo, uint64_t root, uint64_t *total);
 // all staged edges are candidates; else indices in op_cand with count in ctl).
 int tree_add(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total);
 int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total);
+// Split form used to fuse storage and repair into one submission:
+// tree_enqueue (what: 1 add, 2 del) launches without waiting; after the caller
+// has synchronised and read the control block, tree_after_sync finishes it.
+int tree_enqueue(Graph &g, int what, uint64_t n_edges, int directed, bool from_cands);
+int tree_after_sync(Graph &g, int what, uint64_t *total);
 int tree_classify(Graph &g, uint64_t n_edges, int directed, const uint8_t *is_del_dev, uint8_t *unsafe_dev);
 int tree_labels(Graph &g, uint64_t *val, uint64_t *par, uint64_t *pw);
 int tree_checksum(Graph &g, uint64_t *sum);

@@ -214,6 +214,7 @@ __global__ void k_compact(DevDir dir, const void *old_pool, void *new_pool, uint
 
 template <bool W>
 __global__ void k_write_new(DevGraph g, OpView ops, uint64_t nops) {
+  if (g.ctl[C_ERR]) return;  // a failed growth is compacted and replayed by the host
   using E = typename std::conditional<W, uint2, uint32_t>::type;
   E *po = reinterpret_cast<E *>(g.out.pool);
   E *pi = reinterpret_cast<E *>(g.in.pool);
@@ -250,6 +251,7 @@ __device__ __forceinline__ void set_alive(DevDir &dir, uint32_t v, uint32_t pos,
 
 template <bool W>
 __global__ void k_count(DevGraph g, OpView ops, uint64_t nops, int add) {
+  if (g.ctl[C_ERR]) return;
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nops; j += stride) {
     uint32_t rid = ops.rid[j];
@@ -295,6 +297,7 @@ __global__ void k_count(DevGraph g, OpView ops, uint64_t nops, int add) {
 // 0->1 adds (src/sssp_inc_batch.cpp:148) and 1->0 deletes (:166).
 __global__ void k_edge_old(OpView ops, uint64_t n, int directed, int add, int collect, uint64_t *old_out,
                            uint32_t *cand, unsigned long long *ctl) {
+  if (ctl[C_ERR]) return;
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     uint32_t o;
@@ -558,6 +561,7 @@ static int compact_dir(Graph &g, DevDir &dir) {
     cudaFree(dir.owner);
     dir.pool = fresh;
     dir.owner = fresh_owner;
+    g.layout_version++;  // cached level-loop graphs hold the old pool pointers
   }
   cudaFree(tmp);
   cudaFree(offs);
@@ -565,59 +569,86 @@ static int compact_dir(Graph &g, DevDir &dir) {
   return rc;
 }
 
-// Grow the segments that overflowed; if the pool runs out, compact it and
-// grow the rest.
-static int grow_all(Graph &g) {
-  int rc = grow_dir(g, g.d.out, C_GROWN_OUT);
-  if (!rc && !g.symmetric) rc = grow_dir(g, g.d.in, C_GROWN_IN);
-  if (rc) return rc;
-  RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT, cudaMemcpyDeviceToHost, g.stream));
-  RG_CUDA(cudaStreamSynchronize(g.stream));
-  if (g.h_ctl[C_ERR] != RG_ENOSPACE || g.h_ctl[C_AUX] != 1) return RG_OK;
+// Pool exhaustion during growth: compact both directions; the caller then
+// replays the batch from the growth step (storage_replay).
+int storage_recover(Graph &g) {
   RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_ERR], 0, 8, g.stream));
   RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_AUX], 0, 8, g.stream));
-  if ((rc = compact_dir(g, g.d.out))) return rc;
-  if (!g.symmetric && (rc = compact_dir(g, g.d.in))) return rc;
-  rc = grow_dir(g, g.d.out, C_GROWN_OUT);
-  if (!rc && !g.symmetric) rc = grow_dir(g, g.d.in, C_GROWN_IN);
+  int rc = compact_dir(g, g.d.out);
+  if (!rc && !g.symmetric) rc = compact_dir(g, g.d.in);
   return rc;
 }
 
-int storage_add(Graph &g, uint64_t n, uint64_t nops, int directed, uint64_t *old_num, bool collect) {
+static int enqueue_after_lookup(Graph &g, uint64_t n, uint64_t nops, int directed, bool collect) {
   OpView ops = op_view(g);
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_GROWN_OUT], 0, 16, g.stream));
+  int rc = grow_dir(g, g.d.out, C_GROWN_OUT);
+  if (!rc && !g.symmetric) rc = grow_dir(g, g.d.in, C_GROWN_IN);
+  if (rc) return rc;
+  count_launch(g, 3);
   if (collect) RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_CANDN], 0, 8, g.stream));
-  if (nops) {
-    count_launch(g, 4);
-    k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
-    RG_CUDA(cudaGetLastError());
-    int rc = grow_all(g);
-    if (rc) return rc;
-    if (g.weighted) {
-      k_write_new<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
-      k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
-    } else {
-      k_write_new<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
-      k_count<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
-    }
-    k_edge_old<<<grid_for(g, n), TPB, 0, g.stream>>>(ops, n, directed, 1, collect, old_dev(g), op_cand(g), g.d.ctl);
-    RG_CUDA(cudaGetLastError());
+  if (g.weighted) {
+    k_write_new<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
+    k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
+  } else {
+    k_write_new<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops);
+    k_count<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
   }
-  return finish(g, true, old_num, n);
+  k_edge_old<<<grid_for(g, n), TPB, 0, g.stream>>>(ops, n, directed, 1, collect, old_dev(g), op_cand(g), g.d.ctl);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
 }
 
-int storage_del(Graph &g, uint64_t n, uint64_t nops, int directed, uint64_t *old_num, bool collect) {
+// Storage kernels of one staged batch, enqueued without waiting.  Each kernel
+// after the growth step skips its work once the device error word is set.
+int storage_enqueue(Graph &g, bool add, uint64_t n, uint64_t nops, int directed, bool collect) {
   OpView ops = op_view(g);
+  g.adj_version++;
   if (collect) RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_CANDN], 0, 8, g.stream));
-  if (nops) {
-    count_launch(g, 3);
-    k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
-    if (g.weighted) k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
-    else k_count<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
-    k_edge_old<<<grid_for(g, n), TPB, 0, g.stream>>>(ops, n, directed, 0, collect, old_dev(g), op_cand(g), g.d.ctl);
+  if (!nops) return RG_OK;
+  if (add) {
+    RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_GROWN_OUT], 0, 16, g.stream));
+    count_launch(g);
+    k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 1);
     RG_CUDA(cudaGetLastError());
+    return enqueue_after_lookup(g, n, nops, directed, collect);
   }
-  return finish(g, true, old_num, n);
+  count_launch(g, 3);
+  k_lookup<<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+  if (g.weighted) k_count<true><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+  else k_count<false><<<grid_for(g, nops), TPB, 0, g.stream>>>(g.d, ops, nops, 0);
+  k_edge_old<<<grid_for(g, n), TPB, 0, g.stream>>>(ops, n, directed, 0, collect, old_dev(g), op_cand(g), g.d.ctl);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
+}
+
+int storage_replay(Graph &g, uint64_t n, uint64_t nops, int directed, bool collect) {
+  if (!nops) return RG_OK;
+  return enqueue_after_lookup(g, n, nops, directed, collect);
+}
+
+// Per-edge old counts into the pinned staging buffer (read after the sync).
+int storage_copy_old(Graph &g, uint64_t n) {
+  if (n) RG_CUDA(cudaMemcpyAsync(g.stage_host, old_dev(g), n * 8, cudaMemcpyDeviceToHost, g.stream));
+  return RG_OK;
+}
+
+const uint64_t *storage_old_host(Graph &g) { return reinterpret_cast<const uint64_t *>(g.stage_host); }
+
+int sync_ctl(Graph &g) {
+  RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  return RG_OK;
+}
+
+// Device error left by the storage kernels, as a status (clears it).
+int storage_error(Graph &g) {
+  if (!g.h_ctl[C_ERR]) return RG_OK;
+  int code = (int)g.h_ctl[C_ERR];
+  set_error(code == RG_ENOSPACE ? (g.h_ctl[C_AUX] == 1 ? "device edge pool is full" : "device edge index is full")
+                                : "device error");
+  cudaMemsetAsync(&g.d.ctl[C_ERR], 0, 8, g.stream);
+  cudaMemsetAsync(&g.d.ctl[C_AUX], 0, 8, g.stream);
+  return code;
 }
 
 int storage_num(Graph &g, uint64_t nops, uint64_t *num) {

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <type_traits>
 
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "rg_internal.cuh"
@@ -57,13 +59,17 @@ __device__ __forceinline__ uint32_t seg_len(const DevDir &d, uint32_t v) {
 // update_label (core/graph.hpp:1799-1826): CAS {value, parent} while the new
 // value still improves the current one.
 template <int A>
-__device__ __forceinline__ bool relax(ulonglong2 *lab, uint32_t u, uint64_t su, uint32_t v, uint32_t w) {
-  uint64_t nv = Hook<A>::combine(su, w);
-  ulonglong2 cur = ld_lab(&lab[v]);
+__device__ __forceinline__ bool relax(const DevGraph &g, uint32_t u, uint64_t su, uint32_t v, uint32_t w) {
+  const uint64_t nv = Hook<A>::combine(su, w);
+  if (!Hook<A>::better(nv, ld_v32(g.val32, v))) return false;
+  ulonglong2 cur = ld_lab(&g.lab[v]);
   while (Hook<A>::better(nv, cur.x)) {
     ulonglong2 want = make_ulonglong2(nv, pack_parent(u, w));
-    ulonglong2 old = cas128(&lab[v], cur, want);
-    if (old.x == cur.x && old.y == cur.y) return true;
+    ulonglong2 old = cas128(&g.lab[v], cur, want);
+    if (old.x == cur.x && old.y == cur.y) {
+      mirror_improve<A>(g.val32, v, nv);
+      return true;
+    }
     cur = old;
   }
   return false;
@@ -74,7 +80,10 @@ __device__ __forceinline__ void warp_add_result(unsigned long long local, unsign
   if (lane_id() == 0 && local) atomicAdd(dst, local);
 }
 
-__device__ __forceinline__ void mark_modified(const DevGraph &g, bool pred, uint32_t v, uint32_t mst) {
+// Record v in the modified list (trace_modified graphs); the epoch is read
+// from the control block so cached graphs follow rg_clear_modified.
+__device__ __forceinline__ void mark_modified(const DevGraph &g, bool pred, uint32_t v, uint32_t /*on*/) {
+  const uint32_t mst = (uint32_t)g.ctl[C_MODEPOCH];
   bool app = pred && atomicExch(&g.modstamp[v], mst) != mst;
   warp_append(app, v, g.modq, &g.ctl[C_MODN], FULL);
 }
@@ -83,8 +92,10 @@ __device__ __forceinline__ void mark_modified(const DevGraph &g, bool pred, uint
 // push lambdas, core/graph.hpp:910-935, :1017-1042, :1083-1104).
 template <int A, bool W>
 __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
-                                              uint32_t *fout, unsigned long long *fout_n, uint32_t st,
-                                              uint64_t *hubq, unsigned long long *hub_n, uint32_t mst) {
+                                              uint32_t *fout, unsigned long long *fout_n, uint64_t *hubq,
+                                              unsigned long long *hub_n, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_SPARSE) return;
+  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.out.pool);
   const uint64_t n = *fin_n;
@@ -100,7 +111,7 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
       u = fin[i];
       len = seg_len(g.out, u);
       off = g.out.off[u];
-      su = ld_val(&g.lab[u]);
+      su = ld_v32(g.val32, u);
       if (len > HUB) {
         uint32_t nch = (len + CHUNK - 1) / CHUNK;
         unsigned long long k = atomicAdd(hub_n, (unsigned long long)nch);
@@ -136,7 +147,7 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
         uint32_t nb = P::nbr(e);
         if (!(nb & DEAD)) {
           v = nb;
-          upd = relax<A>(g.lab, ou, osu, v, P::wt(e));
+          upd = relax<A>(g,ou, osu, v, P::wt(e));
         }
       }
       local += upd;
@@ -152,8 +163,9 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
 // Hub chunks: CHUNK consecutive slots of one long list per warp iteration.
 template <int A, bool W>
 __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hubq, const unsigned long long *hub_n,
-                                                  uint32_t *fout, unsigned long long *fout_n, uint32_t st,
-                                                  uint32_t mst) {
+                                                  uint32_t *fout, unsigned long long *fout_n, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_SPARSE) return;
+  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.out.pool);
   const uint64_t n = *hub_n;
@@ -166,7 +178,7 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
     const uint32_t u = (uint32_t)task, c = (uint32_t)(task >> 32);
     const uint32_t len = seg_len(g.out, u);
     const uint64_t off = g.out.off[u];
-    const uint64_t su = ld_val(&g.lab[u]);
+    const uint64_t su = ld_v32(g.val32, u);
     const uint32_t start = c * CHUNK, end = min(len, start + CHUNK);
     if (lane == 0 && end > start) scanned += end - start;
     for (uint32_t kb = start; kb < end; kb += 32) {
@@ -178,7 +190,7 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
         uint32_t nb = P::nbr(e);
         if (!(nb & DEAD)) {
           v = nb;
-          upd = relax<A>(g.lab, u, su, v, P::wt(e));
+          upd = relax<A>(g,u, su, v, P::wt(e));
         }
       }
       local += upd;
@@ -199,18 +211,24 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
 template <int A, int N>
 __device__ __forceinline__ void relax_batch(const DevGraph &g, const bool (&on)[N], const uint32_t (&u)[N],
                                             const uint32_t (&v)[N], const uint32_t (&w)[N],
-                                            const uint64_t (&su)[N], ulonglong2 (&cur)[N], uint32_t st,
-                                            uint32_t *fout, unsigned long long *fout_n, unsigned long long &local,
-                                            uint32_t mst) {
+                                            const uint64_t (&su)[N], uint32_t st, uint32_t *fout,
+                                            unsigned long long *fout_n, unsigned long long &local, uint32_t mst) {
   bool pend[N], upd[N];
-  ulonglong2 want[N], old[N];
+  ulonglong2 want[N], old[N], cur[N];
+  uint64_t dv[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) dv[k] = on[k] ? ld_v32(g.val32, v[k]) : 0;
 #pragma unroll
   for (int k = 0; k < N; k++) {
     const uint64_t nv = Hook<A>::combine(su[k], w[k]);
-    pend[k] = on[k] && Hook<A>::better(nv, cur[k].x);
+    pend[k] = on[k] && Hook<A>::better(nv, dv[k]);
     want[k] = make_ulonglong2(nv, pack_parent(u[k], w[k]));
     upd[k] = false;
   }
+#pragma unroll
+  for (int k = 0; k < N; k++) cur[k] = pend[k] ? ld_lab(&g.lab[v[k]]) : make_ulonglong2(0, 0);
+#pragma unroll
+  for (int k = 0; k < N; k++) pend[k] = pend[k] && Hook<A>::better(want[k].x, cur[k].x);
 #pragma unroll
   for (int k = 0; k < N; k++)
     if (pend[k]) old[k] = cas128(&g.lab[v[k]], cur[k], want[k]);
@@ -234,7 +252,10 @@ __device__ __forceinline__ void relax_batch(const DevGraph &g, const bool (&on)[
   uint32_t ex[N];
 #pragma unroll
   for (int k = 0; k < N; k++)
-    if (upd[k]) ex[k] = atomicExch(&g.stamp[v[k]], st);
+    if (upd[k]) {
+      mirror_improve<A>(g.val32, v[k], want[k].x);
+      ex[k] = atomicExch(&g.stamp[v[k]], st);
+    }
   uint32_t cnt = 0;
 #pragma unroll
   for (int k = 0; k < N; k++) {
@@ -276,14 +297,69 @@ constexpr int LB_ITEMS = 4;
 constexpr uint32_t LB_TILE = LB_TPB * LB_ITEMS;
 constexpr uint32_t LB_CAP = 1025;  // staged entries per tile (sparser tiles search P in global memory)
 
-__global__ void k_gather_deg(DevGraph g, const uint32_t *fin, uint64_t n, uint64_t *deg) {
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += stride)
-    deg[i] = i < n ? seg_len(g.out, fin[i]) : 0;
+// Exclusive prefix of the frontier's degrees into P[0..n] (P[n] = total),
+// with n read on the device: every block owns one contiguous range; pass 1
+// sums the ranges, pass 2 scans the range sums in one block, pass 3 scans
+// each range with its offset.
+constexpr int SC_BLOCKS = 512;
+constexpr int SC_TPB = 256;
+
+__device__ __forceinline__ void scan_range(uint64_t n1, int b, uint64_t &lo, uint64_t &hi) {
+  const uint64_t per = (n1 + SC_BLOCKS - 1) / SC_BLOCKS;
+  lo = min(n1, (uint64_t)b * per);
+  hi = min(n1, lo + per);
+}
+
+__global__ void __launch_bounds__(SC_TPB) k_scan_sums(DevGraph g, const uint32_t *fin,
+                                                      const unsigned long long *fin_n, uint64_t *deg,
+                                                      uint64_t *sums) {
+  using BR = cub::BlockReduce<uint64_t, SC_TPB>;
+  __shared__ typename BR::TempStorage tmp;
+  const uint64_t n = *fin_n;
+  uint64_t lo, hi;
+  scan_range(n + 1, blockIdx.x, lo, hi);
+  uint64_t s = 0;
+  for (uint64_t i = lo + threadIdx.x; i < hi; i += SC_TPB) {
+    const uint64_t d = i < n ? seg_len(g.out, fin[i]) : 0;
+    deg[i] = d;
+    s += d;
+  }
+  s = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) sums[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(SC_BLOCKS) k_scan_top(uint64_t *sums) {
+  using BS = cub::BlockScan<uint64_t, SC_BLOCKS>;
+  __shared__ typename BS::TempStorage tmp;
+  uint64_t v = sums[threadIdx.x];
+  BS(tmp).ExclusiveSum(v, v);
+  sums[threadIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(SC_TPB) k_scan_final(const unsigned long long *fin_n, const uint64_t *deg,
+                                                       const uint64_t *sums, uint64_t *P) {
+  using BS = cub::BlockScan<uint64_t, SC_TPB>;
+  __shared__ typename BS::TempStorage tmp;
+  __shared__ uint64_t carry;
+  const uint64_t n = *fin_n;
+  uint64_t lo, hi;
+  scan_range(n + 1, blockIdx.x, lo, hi);
+  if (threadIdx.x == 0) carry = sums[blockIdx.x];
+  __syncthreads();
+  for (uint64_t base = lo; base < hi; base += SC_TPB) {
+    const uint64_t i = base + threadIdx.x;
+    uint64_t d = i < hi ? deg[i] : 0, x, total;
+    BS(tmp).ExclusiveSum(d, x, total);
+    if (i < hi) P[i] = carry + x;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
 }
 
 // tile_lo[t] = last frontier index whose edge range starts at or before t*LB_TILE.
-__global__ void k_partition(const uint64_t *P, uint64_t n, uint32_t *tile_lo) {
+__global__ void k_partition(const uint64_t *P, const unsigned long long *fin_n, uint32_t *tile_lo) {
+  const uint64_t n = *fin_n;
   const uint64_t T = P[n];
   const uint64_t ntiles = (T + LB_TILE - 1) / LB_TILE;
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -300,9 +376,12 @@ __global__ void k_partition(const uint64_t *P, uint64_t n, uint32_t *tile_lo) {
 }
 
 template <int A, bool W>
-__global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32_t *fin, uint64_t n, const uint64_t *P,
+__global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32_t *fin,
+                                                     const unsigned long long *fin_n, const uint64_t *P,
                                                      const uint32_t *tile_lo, uint32_t *fout,
-                                                     unsigned long long *fout_n, uint32_t st, uint32_t mst) {
+                                                     unsigned long long *fout_n, uint32_t mst) {
+  const uint64_t n = *fin_n;
+  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
   using P_ = PoolT<W>;
   const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.out.pool);
   __shared__ uint32_t s_rel[LB_CAP];
@@ -326,7 +405,7 @@ __global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32
         s_rel[j] = pj <= t0 ? 0u : (uint32_t)(pj - t0);
         s_u[j] = u;
         s_base[j] = g.out.off[u] - pj;
-        s_su[j] = ld_val(&g.lab[u]);
+        s_su[j] = ld_v32(g.val32, u);
       }
     }
     __syncthreads();
@@ -360,7 +439,7 @@ __global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32
           uint32_t u = fin[a];
           slot[k] = g.out.off[u] + (e - P[a]);
           uu[k] = u;
-          su[k] = ld_val(&g.lab[u]);
+          su[k] = ld_v32(g.val32, u);
         }
       }
     }
@@ -381,10 +460,7 @@ __global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32
         su[k] = 0;
       }
     }
-    ulonglong2 cur[LB_ITEMS];
-#pragma unroll
-    for (int k = 0; k < LB_ITEMS; k++) cur[k] = on[k] ? ld_lab(&g.lab[vv[k]]) : make_ulonglong2(0, 0);
-    relax_batch<A, LB_ITEMS>(g, on, uu, vv, ww, su, cur, st, fout, fout_n, local, mst);
+    relax_batch<A, LB_ITEMS>(g, on, uu, vv, ww, su, st, fout, fout_n, local, mst);
     __syncthreads();
   }
   warp_add_result(local, &g.ctl[C_RESULT]);
@@ -400,17 +476,21 @@ __global__ void __launch_bounds__(LB_TPB, 3) k_push_lbs(DevGraph g, const uint32
 // search or barrier, and each thread keeps DN_ITEMS slots in flight.
 constexpr int DN_TPB = 256;
 constexpr int DN_ITEMS = 4;
-constexpr uint64_t DENSE_DIV = 20;  // dense when frontier >= V / DENSE_DIV
 
-__global__ void k_mark_active(const uint32_t *fin, uint64_t n, uint32_t *act, uint32_t id) {
+__global__ void k_mark_active(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n, uint32_t *act) {
+  if (g.ctl[C_MODE] != M_DENSE_PUSH) return;
+  const uint32_t id = (uint32_t)g.ctl[C_ACT];
+  const uint64_t n = *fin_n;
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) act[fin[i]] = id;
 }
 
 template <int A, bool W>
-__global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint32_t *act, uint32_t act_id,
-                                                       uint32_t *fout, unsigned long long *fout_n, uint32_t st,
-                                                       uint32_t mst) {
+__global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint32_t *act, uint32_t *fout,
+                                                       unsigned long long *fout_n, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_DENSE_PUSH) return;
+  const uint32_t act_id = (uint32_t)g.ctl[C_ACT];
+  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
   using P_ = PoolT<W>;
   const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.out.pool);
   const uint64_t top = *g.out.pool_top;
@@ -436,20 +516,166 @@ __global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint
       su[k] = 0;
       if (a[k]) {
         typename P_::E ent = __ldg(&pool[base + (uint64_t)k * DN_TPB + threadIdx.x]);
-        su[k] = ld_val(&g.lab[o[k]]);
+        su[k] = ld_v32(g.val32, o[k]);
         vv[k] = P_::nbr(ent);
         ww[k] = P_::wt(ent);
         a[k] = !(vv[k] & DEAD);
         scanned++;
       }
     }
-    ulonglong2 cur[DN_ITEMS];
-#pragma unroll
-    for (int k = 0; k < DN_ITEMS; k++) cur[k] = a[k] ? ld_lab(&g.lab[vv[k]]) : make_ulonglong2(0, 0);
-    relax_batch<A, DN_ITEMS>(g, a, o, vv, ww, su, cur, st, fout, fout_n, local, mst);
+    relax_batch<A, DN_ITEMS>(g, a, o, vv, ww, su, st, fout, fout_n, local, mst);
   }
   warp_add_result(local, &g.ctl[C_RESULT]);
   warp_add_result(scanned, &g.ctl[C_EDGES]);
+}
+
+// ---- dense pull over in-edges ----------------------------------------------
+// The reference's dense mode (stream_edges dense lambda, core/graph.hpp:936-976):
+// every vertex takes the best update_func value over its in-edges.  The whole
+// in-edge range is partitioned once per tree call into PL_TILE-edge tiles
+// (prefix of in-degrees over all vertices, which does not change during the
+// call); a thread reads PL_ITEMS in-edges and their source values, a segmented
+// warp reduction keeps the best candidate per destination, and only the first
+// lane of each destination run issues a CAS.  Per in-edge: one coalesced entry
+// read and one source-value read; no atomics.
+constexpr int PL_TPB = 256;
+constexpr int PL_ITEMS = 4;
+constexpr uint32_t PL_TILE = PL_TPB * PL_ITEMS;
+constexpr uint32_t PL_CAP = PL_TILE + 1;
+
+__global__ void k_in_degrees(DevGraph g, uint64_t *deg) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v <= g.V; v += stride)
+    deg[v] = v < g.V ? seg_len(g.in, (uint32_t)v) : 0;
+}
+
+__global__ void k_in_base(DevGraph g, const uint64_t *P, uint64_t *base) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.V; v += stride)
+    base[v] = g.in.off[v] - P[v];
+}
+
+__global__ void k_partition_tiles(const uint64_t *P, uint64_t n, uint32_t tile_edges, uint32_t *tile_lo) {
+  const uint64_t T = P[n];
+  const uint64_t ntiles = (T + tile_edges - 1) / tile_edges;
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles; t += stride) {
+    uint64_t x = t < ntiles ? t * tile_edges : T;
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(&P[mid]) <= x) lo = mid;
+      else hi = mid - 1;
+    }
+    tile_lo[t] = (uint32_t)(lo < n ? lo : (n ? n - 1 : 0));
+  }
+}
+
+template <int A, bool W>
+__global__ void __launch_bounds__(PL_TPB, 3) k_pull_dense(DevGraph g, const uint64_t *P, const uint64_t *base,
+                                                          const uint32_t *tile_lo, uint32_t *fout,
+                                                          unsigned long long *fout_n, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_PULL) return;
+  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
+  using P_ = PoolT<W>;
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.in.pool);
+  __shared__ uint32_t s_rel[PL_CAP];
+  __shared__ uint64_t s_base[PL_CAP];
+  const uint64_t V = g.V;
+  const uint64_t T = P[V];
+  const uint64_t ntiles = (T + PL_TILE - 1) / PL_TILE;
+  const int lane = lane_id();
+  unsigned long long local = 0;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t t0 = t * PL_TILE;
+    const uint64_t t1 = min(t0 + PL_TILE, T);
+    const uint32_t lo = tile_lo[t];
+    const uint32_t hi = tile_lo[t + 1];
+    const uint32_t m = hi - lo + 1;
+    const bool staged = m <= PL_CAP;
+    if (staged) {
+      for (uint32_t j = threadIdx.x; j < m; j += PL_TPB) {
+        const uint64_t pj = P[lo + j];
+        s_rel[j] = pj <= t0 ? 0u : (uint32_t)(pj - t0);
+        s_base[j] = base[lo + j];
+      }
+    }
+    __syncthreads();
+    uint32_t dv[PL_ITEMS], src[PL_ITEMS], wt[PL_ITEMS];
+    uint64_t cand[PL_ITEMS], sv[PL_ITEMS];
+    bool ok[PL_ITEMS];
+#pragma unroll
+    for (int k = 0; k < PL_ITEMS; k++) {
+      const uint64_t e = t0 + (uint64_t)k * PL_TPB + threadIdx.x;
+      ok[k] = false;
+      dv[k] = NONE;
+      src[k] = 0;
+      wt[k] = 0;
+      if (e < t1) {
+        uint64_t slot;
+        if (staged) {
+          const uint32_t er = (uint32_t)(e - t0);
+          uint32_t a = 0, b = m - 1;
+          while (a < b) {
+            const uint32_t mid = (a + b + 1) >> 1;
+            if (s_rel[mid] <= er) a = mid;
+            else b = mid - 1;
+          }
+          dv[k] = lo + a;
+          slot = s_base[a] + e;
+        } else {
+          uint64_t a = lo, b = hi;
+          while (a < b) {
+            const uint64_t mid = (a + b + 1) >> 1;
+            if (P[mid] <= e) a = mid;
+            else b = mid - 1;
+          }
+          dv[k] = (uint32_t)a;
+          slot = base[a] + e;
+        }
+        const typename P_::E ent = __ldg(&pool[slot]);
+        src[k] = P_::nbr(ent);
+        wt[k] = P_::wt(ent);
+        ok[k] = !(src[k] & DEAD);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PL_ITEMS; k++) sv[k] = ok[k] ? ld_v32(g.val32, src[k]) : 0;
+    bool head[PL_ITEMS];
+#pragma unroll
+    for (int k = 0; k < PL_ITEMS; k++) {
+      // segmented best over the warp's run of equal destinations
+      bool has = ok[k];
+      uint64_t c = has ? Hook<A>::combine(sv[k], wt[k]) : 0;
+      uint32_t s = src[k], w = wt[k];
+      uint64_t su = sv[k];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t odv = __shfl_down_sync(FULL, dv[k], o);
+        const bool ohas = __shfl_down_sync(FULL, has, o);
+        const uint64_t oc = __shfl_down_sync(FULL, c, o);
+        const uint32_t os = __shfl_down_sync(FULL, s, o);
+        const uint32_t ow = __shfl_down_sync(FULL, w, o);
+        const uint64_t osu = __shfl_down_sync(FULL, su, o);
+        if (lane + o < 32 && odv == dv[k] && ohas && (!has || Hook<A>::better(oc, c))) {
+          has = true;
+          c = oc;
+          s = os;
+          w = ow;
+          su = osu;
+        }
+      }
+      const uint32_t pdv = __shfl_up_sync(FULL, dv[k], 1);
+      head[k] = has && dv[k] != NONE && (lane == 0 || pdv != dv[k]);
+      src[k] = s;
+      wt[k] = w;
+      sv[k] = su;
+    }
+    relax_batch<A, PL_ITEMS>(g, head, src, dv, wt, sv, st, fout, fout_n, local, mst);
+    __syncthreads();
+  }
+  warp_add_result(local, &g.ctl[C_RESULT]);
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&g.ctl[C_EDGES], T);
 }
 
 // Bottom-up BFS level for full builds (the reference's dense pull,
@@ -458,7 +684,9 @@ __global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint
 // stopping there.  Used when the frontier is large; each vertex is written
 // only by its own thread, so no atomics on labels.
 template <bool W>
-__global__ void k_bfs_bottom_up(DevGraph g, uint64_t d, uint32_t *fout, unsigned long long *fout_n) {
+__global__ void k_bfs_bottom_up(DevGraph g, uint32_t *fout, unsigned long long *fout_n) {
+  if (g.ctl[C_MODE] != M_BOTTOM_UP) return;
+  const uint64_t d = g.ctl[C_DEPTH];
   using P_ = PoolT<W>;
   const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.in.pool);
   const uint64_t V = g.V;
@@ -467,7 +695,7 @@ __global__ void k_bfs_bottom_up(DevGraph g, uint64_t d, uint32_t *fout, unsigned
   for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < V; base += stride) {
     const uint64_t v = base + threadIdx.x;
     bool found = false;
-    if (v < V && ld_val(&g.lab[v]) == BFS_MAXL) {
+    if (v < V && ld_v32(g.val32, (uint32_t)v) == BFS_MAXL) {
       const uint32_t len = seg_len(g.in, (uint32_t)v);
       const uint64_t off = g.in.off[v];
       for (uint32_t k = 0; k < len; k++) {
@@ -475,8 +703,9 @@ __global__ void k_bfs_bottom_up(DevGraph g, uint64_t d, uint32_t *fout, unsigned
         const uint32_t u = P_::nbr(e);
         scanned++;
         if (u & DEAD) continue;
-        if (ld_val(&g.lab[u]) == d) {
+        if (ld_v32(g.val32, u) == d) {
           g.lab[v] = make_ulonglong2(d + 1, pack_parent(u, P_::wt(e)));
+          g.val32[v] = (uint32_t)(d + 1);
           found = true;
           break;
         }
@@ -489,6 +718,124 @@ __global__ void k_bfs_bottom_up(DevGraph g, uint64_t d, uint32_t *fout, unsigned
   warp_add_result(scanned, &g.ctl[C_EDGES]);
 }
 
+// ---- device-driven level loop ------------------------------------------------
+// A tree call runs k_prologue, its seed kernel, then a CUDA graph whose WHILE
+// node repeats a pair of levels (queue 0 -> 1, then 1 -> 0).  Each level
+// starts with k_level_begin, which reads the frontier size and picks the level
+// mode and stamp on the device; every level kernel returns at once unless the
+// mode is its own; k_loop_cond stops the loop when the frontier is empty.  No
+// host round trip happens between levels (the reference's driver decides
+// between levels on the host, core/graph.hpp:898-983, :1013-1111).
+
+__global__ void k_prologue(DevGraph g, unsigned long long inv_tag) {
+  unsigned long long *c = g.ctl;
+  c[C_INVTAG] = inv_tag;
+  c[C_INVITER] = 0;
+  c[C_QN0] = 0;
+  c[C_QN1] = 0;
+  c[C_HUBN] = 0;
+  c[C_RESULT] = 0;
+  c[C_TREEN] = 0;
+  c[C_RECOMPUTE] = 0;
+  c[C_LEVEL] = 0;
+  c[C_EDGES] = 0;
+  c[C_MODE] = M_EMPTY;
+  c[C_KLAUNCH] = 0;
+  c[C_STAMP] += 1;
+}
+
+// Kernels a level of each mode launches (k_level_begin not included).
+__host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
+  switch (mode) {
+    case M_SPARSE: return 2;
+    case M_PULL: return 1;
+    case M_DENSE_PUSH: return 2;
+    case M_BOTTOM_UP: return 1;
+    case M_LBS: return 5;
+  }
+  return 0;
+}
+
+struct LevelCfg {
+  uint64_t dense_div;
+  uint64_t lbs_min;
+  int allow_pull;
+  int bottom_up;
+};
+
+// Picks the level mode from the frontier size (the reference's push/pull rule
+// at core/graph.hpp:334 and its vertex/edge-centric rule at :595-612 play the
+// same role); inside a graph it also selects the SWITCH case to run.
+__global__ void k_level_begin(DevGraph g, const unsigned long long *fin_n, unsigned long long *fout_n, LevelCfg cfg,
+                              int use_switch, cudaGraphConditionalHandle sw) {
+  unsigned long long *c = g.ctl;
+  const uint64_t n = *fin_n;
+  const uint64_t lvl = c[C_LEVEL];
+  *fout_n = 0;
+  c[C_HUBN] = 0;
+  c[C_STAMP] += 1;
+  c[C_DEPTH] = lvl;
+  const bool dense = n * cfg.dense_div >= g.V;
+  unsigned long long mode = M_SPARSE;
+  if (n == 0) mode = M_EMPTY;
+  else if (dense && cfg.bottom_up) mode = M_BOTTOM_UP;
+  else if (dense && cfg.allow_pull) mode = M_PULL;
+  else if (dense) mode = M_DENSE_PUSH;
+  else if (n >= cfg.lbs_min) mode = M_LBS;
+  if (mode == M_DENSE_PUSH) c[C_ACT] += 1;
+  c[C_MODE] = mode;
+  if (use_switch) c[C_KLAUNCH] += 1 + mode_launches(mode);
+  if (n) {
+    if (lvl < TRACE_CAP) g.trace[lvl] = n;
+    c[C_LEVEL] = lvl + 1;
+  }
+  if (use_switch) cudaGraphSetConditional(sw, (unsigned)mode);
+}
+
+__global__ void k_loop_cond(DevGraph g, const unsigned long long *n_after, uint64_t max_levels,
+                            cudaGraphConditionalHandle handle) {
+  const uint64_t n = *n_after;
+  const uint64_t lvl = g.ctl[C_LEVEL];
+  g.ctl[C_KLAUNCH] += 1;
+  if (n && lvl >= max_levels) atomicCAS(&g.ctl[C_ERR], 0ull, (unsigned long long)RG_ETIMEOUT);
+  cudaGraphSetConditional(handle, (n && lvl < max_levels) ? 1u : 0u);
+}
+
+// Deletion repair loop control (do_update_tree_del, core/graph.hpp:1250-1418):
+// one invalidation level per k_inv_begin; the full-recompute fallback
+// (:1252) stops the loop and turns the rest of the repair into no-ops.
+__global__ void k_inv_begin(DevGraph g, const unsigned long long *fin_n, unsigned long long *fout_n, uint64_t big) {
+  unsigned long long *c = g.ctl;
+  const uint64_t n = *fin_n;
+  *fout_n = 0;
+  c[C_KLAUNCH] += 3;  // this kernel, k_rescue, k_expand
+  if (n == 0 || c[C_RECOMPUTE]) return;
+  const uint64_t it = c[C_INVITER];
+  if (it <= 10 && c[C_TREEN] + n > big) c[C_RECOMPUTE] = 1;
+  c[C_INVITER] = it + 1;
+}
+
+__global__ void k_inv_cond(DevGraph g, const unsigned long long *n_after, uint64_t max_iter,
+                           cudaGraphConditionalHandle handle) {
+  unsigned long long *c = g.ctl;
+  const uint64_t n = *n_after;
+  c[C_KLAUNCH] += 1;
+  cudaGraphSetConditional(handle, (n && !c[C_RECOMPUTE] && c[C_INVITER] < max_iter) ? 1u : 0u);
+}
+
+__global__ void k_copy_frontier(DevGraph g, const uint32_t *src, const unsigned long long *src_n, uint32_t *dst,
+                                unsigned long long *dst_n) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) g.ctl[C_KLAUNCH] += 3;  // k_reset, k_pull, this kernel
+  if (g.ctl[C_RECOMPUTE]) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dst_n = 0;
+    return;
+  }
+  const uint64_t n = *src_n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dst_n = n;
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[i];
+}
+
 // build_tree init (core/graph.hpp:886-896): every label to init_label_func,
 // parent to empty; the active set is the root, or every vertex (WCC).
 template <int A>
@@ -496,8 +843,13 @@ __global__ void k_init(DevGraph g, uint64_t root, uint32_t *fout) {
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.V; v += stride) {
     g.lab[v] = make_ulonglong2(Hook<A>::init(v, root), pack_parent(NONE, 0));
+    g.val32[v] = (uint32_t)Hook<A>::init(v, root);
     if (Hook<A>::all_active) fout[v] = (uint32_t)v;
     else if (v == root) fout[0] = (uint32_t)v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    g.ctl[C_QN0] = Hook<A>::all_active ? g.V : 1;
+    g.ctl[C_ROOT] = root;
   }
 }
 
@@ -506,7 +858,8 @@ __global__ void k_init(DevGraph g, uint64_t root, uint32_t *fout) {
 template <int A>
 __global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, const uint32_t *ow, const uint32_t *cand,
                            const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t *fout,
-                           unsigned long long *fout_n, uint32_t st, uint32_t mst) {
+                           unsigned long long *fout_n, uint32_t mst) {
+  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
   const uint64_t n = cand ? *cand_n : n_all;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -521,7 +874,7 @@ __global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, c
         uint64_t op = directed ? e : 2 * e + dir;
         uint32_t u = os[op];
         v = od[op];
-        upd = relax<A>(g.lab, u, ld_val(&g.lab[u]), v, ow[op]);
+        upd = relax<A>(g,u, ld_v32(g.val32, u), v, ow[op]);
       }
       local += upd;
       bool app = upd && atomicExch(&g.stamp[v], st) != st;
@@ -535,8 +888,9 @@ __global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, c
 // Seeds of update_tree_del (single :1640-1649, batch :1680-1714): a deleted
 // edge that is dst's parent edge invalidates dst.
 __global__ void k_seed_del(DevGraph g, const uint32_t *os, const uint32_t *od, const uint32_t *ow, const uint32_t *cand,
-                           const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t tag_inv,
-                           uint32_t *fout, unsigned long long *fout_n) {
+                           const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t *fout,
+                           unsigned long long *fout_n) {
+  const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   const uint64_t n = cand ? *cand_n : n_all;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -580,7 +934,9 @@ __device__ __forceinline__ bool has_parents(const DevGraph &g, uint32_t x, uint3
 // moves to that in-edge.  One warp per frontier vertex.
 template <int A, bool W>
 __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
-                                                uint32_t tag_inv, uint64_t limit) {
+                                                uint64_t limit) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
   const uint64_t n = *fin_n;
@@ -590,7 +946,7 @@ __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin,
   for (uint64_t idx = warp; idx < n; idx += nwarps) {
     const uint32_t d = fin[idx];
     if (ld_u32(&g.inv[d]) != tag_inv) continue;
-    const uint64_t sd = ld_val(&g.lab[d]);
+    const uint64_t sd = ld_v32(g.val32, d);
     const uint32_t len = seg_len(g.in, d);
     const uint64_t off = g.in.off[d];
     for (uint32_t kb = 0; kb < len; kb += 32) {
@@ -601,7 +957,7 @@ __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin,
         typename P::E e = pool[off + k];
         src = P::nbr(e);
         w = P::wt(e);
-        if (!(src & DEAD) && Hook<A>::combine(ld_val(&g.lab[src]), w) == sd) ok = !has_parents(g, src, tag_inv, limit);
+        if (!(src & DEAD) && Hook<A>::combine(ld_v32(g.val32, src), w) == sd) ok = !has_parents(g, src, tag_inv, limit);
       }
       unsigned b = __ballot_sync(FULL, ok);
       bool done = false;
@@ -625,8 +981,9 @@ __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin,
 // the reset set; its tree children (parent == (u,w)) are invalidated next.
 template <int A, bool W>
 __global__ void __launch_bounds__(TPB) k_expand(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
-                                                uint32_t *tree, uint32_t *fout, unsigned long long *fout_n,
-                                                uint32_t tag_inv) {
+                                                uint32_t *tree, uint32_t *fout, unsigned long long *fout_n) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.out.pool);
   const uint64_t n = *fin_n;
@@ -661,8 +1018,9 @@ __global__ void __launch_bounds__(TPB) k_expand(DevGraph g, const uint32_t *fin,
 
 // Reset the invalid set to init (core/graph.hpp:1420-1430).
 template <int A>
-__global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long long *tree_n, uint64_t root,
-                        uint32_t mst) {
+__global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long long *tree_n, uint32_t mst) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint64_t root = g.ctl[C_ROOT];
   const uint64_t n = *tree_n;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -672,6 +1030,7 @@ __global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long lo
     if (i < n) {
       u = tree[i];
       g.lab[u] = make_ulonglong2(Hook<A>::init(u, root), pack_parent(NONE, 0));
+      g.val32[u] = (uint32_t)Hook<A>::init(u, root);
     }
     if (mst) mark_modified(g, i < n, u, mst);
   }
@@ -682,6 +1041,7 @@ __global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long lo
 template <int A, bool W>
 __global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
                                               uint32_t mst) {
+  if (g.ctl[C_RECOMPUTE]) return;
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
   const uint64_t n = *fin_n;
@@ -693,13 +1053,13 @@ __global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, c
     const uint32_t d = fin[idx];
     const uint32_t len = seg_len(g.in, d);
     const uint64_t off = g.in.off[d];
-    uint64_t best = ld_val(&g.lab[d]), bsu = 0;
+    uint64_t best = ld_v32(g.val32, d), bsu = 0;
     uint32_t bsrc = NONE, bw = 0;
     for (uint32_t k = lane; k < len; k += 32) {
       typename P::E e = pool[off + k];
       uint32_t s = P::nbr(e);
       if (s & DEAD) continue;
-      uint64_t su = ld_val(&g.lab[s]);
+      uint64_t su = ld_v32(g.val32, s);
       uint64_t nv = Hook<A>::combine(su, P::wt(e));
       if (Hook<A>::better(nv, best)) { best = nv; bsrc = s; bw = P::wt(e); bsu = su; }
     }
@@ -712,7 +1072,7 @@ __global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, c
       if (os != NONE && (bsrc == NONE || Hook<A>::better(ob, best))) { best = ob; bsu = osu; bsrc = os; bw = ow; }
     }
     bool upd = false;
-    if (lane == 0 && bsrc != NONE) upd = relax<A>(g.lab, bsrc, bsu, d, bw);
+    if (lane == 0 && bsrc != NONE) upd = relax<A>(g,bsrc, bsu, d, bw);
     local += upd;
     if (mst) mark_modified(g, __shfl_sync(FULL, upd, 0) && lane == 0, d, mst);
   }
@@ -732,7 +1092,7 @@ __global__ void k_classify(DevGraph g, const uint32_t *os, const uint32_t *od, c
       uint64_t op = directed ? i : 2 * i + dir;
       uint32_t u = os[op], v = od[op], w = ow[op];
       if (del) r = r || ld_meta(&g.lab[v]) == pack_parent(u, w);
-      else r = r || Hook<A>::better(Hook<A>::combine(ld_val(&g.lab[u]), w), ld_val(&g.lab[v]));
+      else r = r || Hook<A>::better(Hook<A>::combine(ld_v32(g.val32, u), w), ld_val(&g.lab[v]));
     }
     unsafe[i] = r;
   }
@@ -767,15 +1127,7 @@ int grid_warps(const Graph &g, uint64_t warps) {
   return (int)(b ? b : 1);
 }
 
-uint32_t next_stamp(Graph &g) {
-  if (++g.stamp_epoch == 0xFFFFFFFFu) {
-    cudaMemsetAsync(g.d.stamp, 0, (size_t)g.V * 4, g.stream);
-    g.stamp_epoch = 1;
-  }
-  return g.stamp_epoch;
-}
-
-uint32_t mod_stamp(Graph &g) { return g.trace ? g.mod_epoch : 0u; }
+uint32_t mod_stamp(Graph &g) { return g.trace ? 1u : 0u; }
 
 int read_ctl(Graph &g) {
   RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT, cudaMemcpyDeviceToHost, g.stream));
@@ -783,189 +1135,394 @@ int read_ctl(Graph &g) {
   return RG_OK;
 }
 
-// Push levels to a fixpoint from the frontier (fin, *fin_n) with n0 entries
-// (do_update_tree_add, core/graph.hpp:1013-1111; build_tree :898-983).
+// Stamps and dense-level activity ids count up on the device, one per level.
+// A call runs at most max_levels levels, so clearing the arrays whenever the
+// last observed counter is within that margin of 2^32 keeps them unique.
+int guard_counters(Graph &g) {
+  const uint64_t margin = 8 * (uint64_t)g.V + (1ull << 16);
+  if (g.h_ctl[C_STAMP] + margin >= 0xFFFFFFFFull) {
+    RG_CUDA(cudaMemsetAsync(g.d.stamp, 0, (size_t)g.V * 4 + 4, g.stream));
+    RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_STAMP], 0, 8, g.stream));
+    g.h_ctl[C_STAMP] = 0;
+  }
+  if (g.h_ctl[C_ACT] + margin >= 0xFFFFFFFFull) {
+    RG_CUDA(cudaMemsetAsync(g.act, 0, (size_t)g.V * 4 + 4, g.stream));
+    RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_ACT], 0, 8, g.stream));
+    g.h_ctl[C_ACT] = 0;
+  }
+  return RG_OK;
+}
+
+// In-edge partition for dense pull levels, rebuilt only after the adjacency changed.
+int prepare_pull(Graph &g) {
+  if (!g.dense_pull || g.pull_version == g.adj_version) return RG_OK;
+  count_launch(g, 5);
+  k_in_degrees<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.scratch64);
+  size_t tb = g.cub_tmp_bytes;
+  RG_CUDA(cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.pull_P, g.V + 1, g.stream));
+  k_in_base<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.pull_P, g.pull_base);
+  k_partition_tiles<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.pull_P, g.V, PL_TILE, g.pull_tile);
+  RG_CUDA(cudaGetLastError());
+  g.pull_version = g.adj_version;
+  return RG_OK;
+}
+
+uint64_t max_levels_of(const Graph &g) { return 4 * (uint64_t)g.V + 1024; }
+
+// Kernels of one level mode for one half-level (queue half -> queue half^1).
 template <int A, bool W>
-int push_levels(Graph &g, const uint32_t *fin, unsigned long long *fin_n, uint64_t n0, bool bfs_levels = false) {
-  const uint32_t *cur = fin;
-  unsigned long long *cur_n = fin_n;
-  uint64_t n = n0;
+int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
+  const uint32_t *fin = g.q[half];
+  unsigned long long *fin_n = &g.d.ctl[C_QN0 + half];
+  uint32_t *fout = g.q[half ^ 1];
+  unsigned long long *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
   unsigned long long *hub_n = &g.d.ctl[C_HUBN];
-  // Values move monotonically, so levels are bounded; the cap only turns a
-  // logic error into a status instead of an endless loop.
-  const uint64_t max_levels = 4 * (uint64_t)g.V + 1024;
-  for (uint64_t lvl = 0; n; lvl++) {
-    if (lvl > max_levels) {
+  const uint32_t mst = mod_stamp(g);
+  switch (mode) {
+    case M_SPARSE:
+      k_push<A, W><<<g.num_sms * 16, TPB, 0, s>>>(g.d, fin, fin_n, fout, fout_n, g.hubq, hub_n, mst);
+      k_push_hub<A, W><<<g.num_sms * 8, TPB, 0, s>>>(g.d, g.hubq, hub_n, fout, fout_n, mst);
+      break;
+    case M_PULL:
+      k_pull_dense<A, W><<<g.num_sms * 3, PL_TPB, 0, s>>>(g.d, g.pull_P, g.pull_base, g.pull_tile, fout, fout_n, mst);
+      break;
+    case M_DENSE_PUSH:
+      k_mark_active<<<g.num_sms * 8, TPB, 0, s>>>(g.d, fin, fin_n, g.act);
+      k_push_dense<A, W><<<g.num_sms * 3, DN_TPB, 0, s>>>(g.d, g.act, fout, fout_n, mst);
+      break;
+    case M_BOTTOM_UP:
+      k_bfs_bottom_up<W><<<g.num_sms * 8, TPB, 0, s>>>(g.d, fout, fout_n);
+      break;
+    case M_LBS:
+      k_scan_sums<<<SC_BLOCKS, SC_TPB, 0, s>>>(g.d, fin, fin_n, g.scratch64, g.lb_sums);
+      k_scan_top<<<1, SC_BLOCKS, 0, s>>>(g.lb_sums);
+      k_scan_final<<<SC_BLOCKS, SC_TPB, 0, s>>>(fin_n, g.scratch64, g.lb_sums, g.lb_P);
+      k_partition<<<g.num_sms * 4, TPB, 0, s>>>(g.lb_P, fin_n, g.lb_tile);
+      k_push_lbs<A, W><<<g.num_sms * 3, LB_TPB, 0, s>>>(g.d, fin, fin_n, g.lb_P, g.lb_tile, fout, fout_n, mst);
+      break;
+    default:
+      break;
+  }
+  return cudaGetLastError() == cudaSuccess ? RG_OK : RG_ECUDA;
+}
+
+LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
+  LevelCfg cfg;
+  cfg.dense_div = g.dense_div;
+  cfg.lbs_min = g.lbs_min;
+  cfg.allow_pull = (build_variant && g.dense_pull) ? 1 : 0;
+  cfg.bottom_up = (A == RG_BFS && build_variant && g.bfs_bottom_up) ? 1 : 0;
+  return cfg;
+}
+
+// The level loop as a CUDA graph:
+//   WHILE (frontier non-empty) {
+//     k_level_begin(q0 -> q1) ; SWITCH(mode) { sparse | pull | dense push | bottom-up | edge-balanced }
+//     k_level_begin(q1 -> q0) ; SWITCH(mode) { ... }
+//     k_loop_cond
+//   }
+// Built once per (algorithm, weighting, variant) and cached until the pool is
+// relocated by a compaction or an option changes.
+template <int A, bool W>
+int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
+  const LevelCfg cfg = level_cfg(g, A, build_variant);
+  LoopGraph &slot = g.loops[(A * 2 + (W ? 1 : 0)) * 2 + (build_variant ? 1 : 0)];
+  const uint64_t key = (g.layout_version << 40) ^ (cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^
+                       ((uint64_t)cfg.allow_pull << 1) ^ (uint64_t)cfg.bottom_up;
+  if (slot.exec && slot.key == key) {
+    *out = slot.exec;
+    return RG_OK;
+  }
+  if (slot.exec) {
+    cudaGraphExecDestroy(slot.exec);
+    slot.exec = nullptr;
+  }
+  if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
+  cudaGraph_t graph;
+  RG_CUDA(cudaGraphCreate(&graph, 0));
+  int rc = RG_OK;
+  cudaError_t e = cudaSuccess;
+  do {
+    cudaGraphConditionalHandle wh;
+    if ((e = cudaGraphConditionalHandleCreate(&wh, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = wh;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    if ((e = cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp)) != cudaSuccess) break;
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    cudaGraphNode_t prev = nullptr;
+    for (int half = 0; half < 2 && e == cudaSuccess && !rc; half++) {
+      cudaGraphConditionalHandle sw;
+      if ((e = cudaGraphConditionalHandleCreate(&sw, body, 0, 0)) != cudaSuccess) break;
+      const unsigned long long *fin_n = &g.d.ctl[C_QN0 + half];
+      unsigned long long *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
+      int use_switch = 1;
+      LevelCfg c = cfg;
+      void *args[] = {(void *)&g.d, (void *)&fin_n, (void *)&fout_n, (void *)&c, (void *)&use_switch, (void *)&sw};
+      cudaKernelNodeParams kp = {};
+      kp.func = (void *)k_level_begin;
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(1);
+      kp.kernelParams = args;
+      cudaGraphNode_t kn;
+      if ((e = cudaGraphAddKernelNode(&kn, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp)) != cudaSuccess) break;
+      cudaGraphNodeParams sp = {};
+      sp.type = cudaGraphNodeTypeConditional;
+      sp.conditional.handle = sw;
+      sp.conditional.type = cudaGraphCondTypeSwitch;
+      sp.conditional.size = M_COUNT;
+      cudaGraphNode_t sn;
+      if ((e = cudaGraphAddNode(&sn, body, &kn, 1, &sp)) != cudaSuccess) break;
+      for (unsigned long long m = 1; m < M_COUNT && e == cudaSuccess && !rc; m++) {
+        if (m == M_PULL && !cfg.allow_pull) continue;
+        if (m == M_BOTTOM_UP && !cfg.bottom_up) continue;
+        cudaGraph_t cg = sp.conditional.phGraph_out[m];
+        if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, cg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+            cudaSuccess)
+          break;
+        rc = enqueue_mode<A, W>(g, g.cap_stream, half, m);
+        e = cudaStreamEndCapture(g.cap_stream, &cg);
+      }
+      prev = sn;
+    }
+    if (e != cudaSuccess || rc) break;
+    const unsigned long long *n_after = &g.d.ctl[C_QN0];
+    uint64_t maxl = max_levels_of(g);
+    void *cargs[] = {(void *)&g.d, (void *)&n_after, (void *)&maxl, (void *)&wh};
+    cudaKernelNodeParams cp = {};
+    cp.func = (void *)k_loop_cond;
+    cp.gridDim = dim3(1);
+    cp.blockDim = dim3(1);
+    cp.kernelParams = cargs;
+    cudaGraphNode_t cn;
+    if ((e = cudaGraphAddKernelNode(&cn, body, &prev, 1, &cp)) != cudaSuccess) break;
+    e = cudaGraphInstantiate(&slot.exec, graph, 0);
+  } while (0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    slot.exec = nullptr;
+    return cuda_fail(e, "building the level-loop graph");
+  }
+  if (rc) return rc;
+  slot.key = key;
+  *out = slot.exec;
+  return RG_OK;
+}
+
+// Push levels to a fixpoint from the frontier in queue 0 (do_update_tree_add,
+// core/graph.hpp:1013-1111; build_tree :898-983).  Enqueues one graph launch;
+// with profiling on, the host runs the same kernels level by level (syncing)
+// so each level can be timed.
+template <int A, bool W>
+int push_levels(Graph &g, bool build_variant) {
+  if (build_variant) {
+    int rc = prepare_pull(g);
+    if (rc) return rc;
+  }
+  if (!g.profiling) {
+    cudaGraphExec_t exec;
+    int rc = loop_exec<A, W>(g, build_variant, &exec);
+    if (rc) return rc;
+    RG_CUDA(cudaGraphLaunch(exec, g.stream));
+    return RG_OK;
+  }
+  const LevelCfg cfg = level_cfg(g, A, build_variant);
+  int rc = read_ctl(g);
+  if (rc) return rc;
+  for (int half = 0; g.h_ctl[C_QN0 + half]; half ^= 1) {
+    if (g.h_ctl[C_LEVEL] >= max_levels_of(g)) {
       set_error("push levels did not converge");
       return RG_ETIMEOUT;
     }
-    g.st_frontier.push_back(n);
-    int nb = (cur == g.q[0]) ? 1 : 0;
-    uint32_t *next = g.q[nb];
-    unsigned long long *next_n = &g.d.ctl[C_QN0 + nb];
-    RG_CUDA(cudaMemsetAsync(next_n, 0, 8, g.stream));
-    RG_CUDA(cudaMemsetAsync(hub_n, 0, 8, g.stream));
-    uint32_t st = next_stamp(g);
-    if (g.profiling) RG_CUDA(cudaEventRecord(g.pev[0], g.stream));
-    if (A == RG_BFS && bfs_levels && n * DENSE_DIV >= g.V) {
-      // full BFS build: the frontier is exactly depth lvl; pull bottom-up
-      count_launch(g);
-      k_bfs_bottom_up<W><<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, lvl, next, next_n);
-    } else if (n * DENSE_DIV >= g.V) {
-      if (++g.act_epoch == 0xFFFFFFFFu) {
-        RG_CUDA(cudaMemsetAsync(g.act, 0, (size_t)g.V * 4, g.stream));
-        g.act_epoch = 1;
-      }
-      count_launch(g, 2);
-      k_mark_active<<<grid_warps(g, (n + 31) / 32), TPB, 0, g.stream>>>(cur, n, g.act, g.act_epoch);
-      k_push_dense<A, W><<<g.num_sms * 3, DN_TPB, 0, g.stream>>>(g.d, g.act, g.act_epoch, next, next_n, st,
-                                                                 mod_stamp(g));
-    } else if (n >= LBS_MIN_FRONTIER) {
-      count_launch(g, 4);
-      k_gather_deg<<<grid_warps(g, (n + 32) / 32), TPB, 0, g.stream>>>(g.d, cur, n, g.scratch64);
-      size_t tb = g.cub_tmp_bytes;
-      RG_CUDA(cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.lb_P, n + 1, g.stream));
-      k_partition<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.lb_P, n, g.lb_tile);
-      k_push_lbs<A, W><<<g.num_sms * 3, LB_TPB, 0, g.stream>>>(g.d, cur, n, g.lb_P, g.lb_tile, next, next_n, st,
-                                                               mod_stamp(g));
-    } else {
-      count_launch(g, 2);
-      k_push<A, W><<<grid_warps(g, (n + 31) / 32), TPB, 0, g.stream>>>(g.d, cur, cur_n, next, next_n, st, g.hubq,
-                                                                        hub_n, mod_stamp(g));
-      k_push_hub<A, W><<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.hubq, hub_n, next, next_n, st, mod_stamp(g));
+    RG_CUDA(cudaEventRecord(g.pev[0], g.stream));
+    count_launch(g);
+    k_level_begin<<<1, 1, 0, g.stream>>>(g.d, &g.d.ctl[C_QN0 + half], &g.d.ctl[C_QN0 + (half ^ 1)], cfg, 0,
+                                          cudaGraphConditionalHandle{});
+    if ((rc = read_ctl(g))) return rc;
+    const unsigned long long mode = g.h_ctl[C_MODE];
+    count_launch(g, mode_launches(mode));
+    if ((rc = enqueue_mode<A, W>(g, g.stream, half, mode))) return rc;
+    RG_CUDA(cudaEventRecord(g.pev[1], g.stream));
+    if ((rc = read_ctl(g))) return rc;
+    float ms = 0.f;
+    RG_CUDA(cudaEventElapsedTime(&ms, g.pev[0], g.pev[1]));
+    g.prof_ms += ms;
+    g.prof_launches += 1;
+    g.st_level_ms.push_back(ms);
+  }
+  return RG_OK;
+}
+
+uint64_t recompute_threshold(const Graph &g) {
+  return std::max<uint64_t>((uint64_t)(0.05 * (double)g.V), g.recompute_min);
+}
+
+// Deletion repair as a graph (do_update_tree_del, core/graph.hpp:1235-1612):
+//   WHILE (invalidated frontier non-empty and no recompute) {
+//     k_inv_begin ; k_rescue ; k_expand     (queue 0 -> 1)
+//     k_inv_begin ; k_rescue ; k_expand     (queue 1 -> 0)
+//     k_inv_cond }
+//   k_reset ; k_pull ; k_copy_frontier (reset set -> queue 0 for the push loop)
+template <int A, bool W>
+int del_exec(Graph &g, cudaGraphExec_t *out) {
+  LoopGraph &slot = g.dels[A * 2 + (W ? 1 : 0)];
+  const uint64_t big = recompute_threshold(g);
+  const uint64_t key = (g.layout_version << 40) ^ big;
+  if (slot.exec && slot.key == key) {
+    *out = slot.exec;
+    return RG_OK;
+  }
+  if (slot.exec) {
+    cudaGraphExecDestroy(slot.exec);
+    slot.exec = nullptr;
+  }
+  if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
+  const uint64_t limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
+  const uint32_t mst = mod_stamp(g);
+  const int gridw = g.num_sms * 16;
+  cudaGraph_t graph;
+  RG_CUDA(cudaGraphCreate(&graph, 0));
+  cudaError_t e = cudaSuccess;
+  do {
+    cudaGraphConditionalHandle wh;
+    if ((e = cudaGraphConditionalHandleCreate(&wh, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = wh;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    if ((e = cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp)) != cudaSuccess) break;
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+        cudaSuccess)
+      break;
+    for (int half = 0; half < 2; half++) {
+      unsigned long long *fin_n = &g.d.ctl[C_QN0 + half], *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
+      k_inv_begin<<<1, 1, 0, g.cap_stream>>>(g.d, fin_n, fout_n, big);
+      k_rescue<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, limit);
+      k_expand<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
     }
-    RG_CUDA(cudaGetLastError());
-    if (g.profiling) RG_CUDA(cudaEventRecord(g.pev[1], g.stream));
-    int rc = read_ctl(g);
-    if (rc) return rc;
-    if (g.profiling) {
-      float ms = 0.f;
-      RG_CUDA(cudaEventElapsedTime(&ms, g.pev[0], g.pev[1]));
-      g.prof_ms += ms;
-      g.prof_launches += 1;
-      g.st_level_ms.push_back(ms);
+    k_inv_cond<<<1, 1, 0, g.cap_stream>>>(g.d, &g.d.ctl[C_QN0], (uint64_t)g.V + 2, wh);
+    e = cudaStreamEndCapture(g.cap_stream, &body);
+    if (e != cudaSuccess) break;
+    if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, graph, &wnode, nullptr, 1, cudaStreamCaptureModeRelaxed)) !=
+        cudaSuccess)
+      break;
+    k_reset<A><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
+    k_pull<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
+    k_copy_frontier<<<g.num_sms * 4, TPB, 0, g.cap_stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], g.q[0], &g.d.ctl[C_QN0]);
+    cudaGraph_t g2 = graph;
+    e = cudaStreamEndCapture(g.cap_stream, &g2);
+    if (e != cudaSuccess) break;
+    e = cudaGraphInstantiate(&slot.exec, graph, 0);
+  } while (0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    slot.exec = nullptr;
+    return cuda_fail(e, "building the deletion-repair graph");
+  }
+  slot.key = key;
+  *out = slot.exec;
+  return RG_OK;
+}
+
+template <int A, bool W>
+int build_enqueue(Graph &g, uint64_t root) {
+  int rc = guard_counters(g);
+  if (rc) return rc;
+  count_launch(g, 2);
+  k_prologue<<<1, 1, 0, g.stream>>>(g.d, 0ull);
+  k_init<A><<<g.num_sms * 16, TPB, 0, g.stream>>>(g.d, root, g.q[0]);
+  RG_CUDA(cudaGetLastError());
+  return push_levels<A, W>(g, true);
+}
+
+template <int A, bool W>
+int add_enqueue(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
+  int rc = guard_counters(g);
+  if (rc) return rc;
+  count_launch(g, 2);
+  k_prologue<<<1, 1, 0, g.stream>>>(g.d, 0ull);
+  k_seed_add<A><<<grid_warps(g, (n_edges + 31) / 32), TPB, 0, g.stream>>>(
+      g.d, op_src(g), op_dst(g), op_w(g), from_cands ? op_cand(g) : nullptr, &g.d.ctl[C_CANDN], n_edges, directed,
+      g.q[0], &g.d.ctl[C_QN0], mod_stamp(g));
+  RG_CUDA(cudaGetLastError());
+  return push_levels<A, W>(g, false);
+}
+
+template <int A, bool W>
+int del_enqueue(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
+  int rc = guard_counters(g);
+  if (rc) return rc;
+  if (++g.inv_epoch >= 0x7FFFFFFFu) {
+    RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+    g.inv_epoch = 1;
+  }
+  const unsigned long long tag = 2ull * g.inv_epoch;  // tag: invalidated; tag+1: rescued
+  count_launch(g, 2);
+  k_prologue<<<1, 1, 0, g.stream>>>(g.d, tag);
+  k_seed_del<<<grid_warps(g, (n_edges + 31) / 32), TPB, 0, g.stream>>>(
+      g.d, op_src(g), op_dst(g), op_w(g), from_cands ? op_cand(g) : nullptr, &g.d.ctl[C_CANDN], n_edges, directed,
+      g.q[0], &g.d.ctl[C_QN0]);
+  RG_CUDA(cudaGetLastError());
+  cudaGraphExec_t exec;
+  if ((rc = del_exec<A, W>(g, &exec))) return rc;
+  RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  return push_levels<A, W>(g, false);
+}
+
+// After the stream has been synchronised and h_ctl read: errors, statistics
+// and the full-recompute fallback of a deletion repair.
+template <int A, bool W>
+int after_sync(Graph &g, int what) {
+  if (g.h_ctl[C_ERR]) {
+    int code = (int)g.h_ctl[C_ERR];
+    set_error(code == RG_ETIMEOUT ? "push levels did not converge" : "device error in tree update");
+    cudaMemsetAsync(&g.d.ctl[C_ERR], 0, 8, g.stream);
+    return code;
+  }
+  g.launches += g.h_ctl[C_KLAUNCH];  // kernels run inside graphs, counted on the device
+  g.st_levels = g.h_ctl[C_LEVEL];
+  if (what == 2) {
+    g.st_invalidated = g.h_ctl[C_TREEN];
+    if (g.h_ctl[C_RECOMPUTE]) {
+      g.st_recomputes++;
+      RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+      g.inv_epoch = 0;
+      int rc = build_enqueue<A, W>(g, g.root);
+      if (!rc) rc = read_ctl(g);
+      if (!rc) rc = after_sync<A, W>(g, 0);
+      return rc;
     }
-    n = g.h_ctl[C_QN0 + nb];
-    cur = next;
-    cur_n = next_n;
-    g.st_levels++;
   }
   return RG_OK;
 }
 
 template <int A, bool W>
-int build_impl(Graph &g, uint64_t root) {
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_RESULT], 0, 8, g.stream));
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_QN0], 0, 8, g.stream));
-  count_launch(g);
-  k_init<A><<<g.num_sms * 16, TPB, 0, g.stream>>>(g.d, root, g.q[0]);
-  RG_CUDA(cudaGetLastError());
-  uint64_t n0 = Hook<A>::all_active ? g.V : 1;
-  unsigned long long hn = n0;
-  RG_CUDA(cudaMemcpyAsync(&g.d.ctl[C_QN0], &hn, 8, cudaMemcpyHostToDevice, g.stream));
-  RG_CUDA(cudaStreamSynchronize(g.stream));
-  if (g.trace) {
-    // every label is rewritten; the modified list becomes "all vertices" lazily
-    // through the same dedup stamps.
-  }
-  return push_levels<A, W>(g, g.q[0], &g.d.ctl[C_QN0], n0, /*bfs_levels=*/true);
-}
-
-template <int A, bool W>
-int add_impl(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_RESULT], 0, 8, g.stream));
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_QN0], 0, 8, g.stream));
-  uint32_t st = next_stamp(g);
-  count_launch(g);
-  k_seed_add<A><<<grid_warps(g, (n_edges + 31) / 32), TPB, 0, g.stream>>>(
-      g.d, op_src(g), op_dst(g), op_w(g), from_cands ? op_cand(g) : nullptr, &g.d.ctl[C_CANDN], n_edges, directed,
-      g.q[0], &g.d.ctl[C_QN0], st, mod_stamp(g));
-  RG_CUDA(cudaGetLastError());
-  int rc = read_ctl(g);
-  if (rc) return rc;
-  return push_levels<A, W>(g, g.q[0], &g.d.ctl[C_QN0], g.h_ctl[C_QN0]);
-}
-
-template <int A, bool W>
-int del_impl(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_RESULT], 0, 8, g.stream));
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_QN0], 0, 8, g.stream));
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_TREEN], 0, 8, g.stream));
-  RG_CUDA(cudaMemsetAsync(&g.d.ctl[C_RECOMPUTE], 0, 8, g.stream));
-  if (++g.inv_epoch >= 0x7FFFFFFFu) {
-    RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
-    g.inv_epoch = 1;
-  }
-  const uint32_t tag = 2 * g.inv_epoch;   // tag: invalidated; tag+1: rescued
-  count_launch(g);
-  k_seed_del<<<grid_warps(g, (n_edges + 31) / 32), TPB, 0, g.stream>>>(
-      g.d, op_src(g), op_dst(g), op_w(g), from_cands ? op_cand(g) : nullptr, &g.d.ctl[C_CANDN], n_edges, directed, tag,
-      g.q[0], &g.d.ctl[C_QN0]);
-  RG_CUDA(cudaGetLastError());
-  int rc = read_ctl(g);
-  if (rc) return rc;
-  uint64_t n = g.h_ctl[C_QN0];
-  if (n == 0) return RG_OK;
-  const uint64_t limit = (uint64_t)((double)g.V * 0.1);
-  const uint64_t big = std::max<uint64_t>((uint64_t)(0.05 * (double)g.V), 2000000);
-  const uint32_t *cur = g.q[0];
-  unsigned long long *cur_n = &g.d.ctl[C_QN0];
-  bool recompute = false;
-  for (uint64_t i = 0; n; i++) {
-    // full recompute fallback (core/graph.hpp:1252)
-    if (i <= 10 && g.h_ctl[C_TREEN] + n > big) { recompute = true; break; }
-    int nb = (cur == g.q[0]) ? 1 : 0;
-    uint32_t *next = g.q[nb];
-    unsigned long long *next_n = &g.d.ctl[C_QN0 + nb];
-    RG_CUDA(cudaMemsetAsync(next_n, 0, 8, g.stream));
-    count_launch(g, 2);
-    k_rescue<A, W><<<grid_warps(g, n), TPB, 0, g.stream>>>(g.d, cur, cur_n, tag, limit);
-    k_expand<A, W><<<grid_warps(g, n), TPB, 0, g.stream>>>(g.d, cur, cur_n, g.tree, next, next_n, tag);
-    RG_CUDA(cudaGetLastError());
-    if ((rc = read_ctl(g))) return rc;
-    if (g.h_ctl[C_RECOMPUTE]) { recompute = true; break; }
-    n = g.h_ctl[C_QN0 + nb];
-    cur = next;
-    cur_n = next_n;
-    g.st_levels++;
-  }
-  if (recompute) {
-    g.st_recomputes++;
-    uint64_t keep = 0;
-    RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
-    g.inv_epoch = 0;
-    (void)keep;
-    return build_impl<A, W>(g, g.root);
-  }
-  uint64_t nt = g.h_ctl[C_TREEN];
-  g.st_invalidated += nt;
-  if (nt == 0) return RG_OK;
-  count_launch(g, 2);
-  k_reset<A><<<grid_warps(g, (nt + 31) / 32), TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], g.root,
-                                                                   mod_stamp(g));
-  k_pull<A, W><<<grid_warps(g, nt), TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mod_stamp(g));
-  RG_CUDA(cudaGetLastError());
-  return push_levels<A, W>(g, g.tree, &g.d.ctl[C_TREEN], nt);
+int run_what(Graph &g, int what, uint64_t a, int directed, bool from_cands, int phase) {
+  if (phase == 1) return after_sync<A, W>(g, what);
+  if (what == 0) return build_enqueue<A, W>(g, a);
+  if (what == 1) return add_enqueue<A, W>(g, a, directed, from_cands);
+  return del_enqueue<A, W>(g, a, directed, from_cands);
 }
 
 template <int A>
-int dispatch_w(Graph &g, int what, uint64_t a, int directed, bool from_cands) {
-  if (g.weighted) {
-    if (what == 0) return build_impl<A, true>(g, a);
-    if (what == 1) return add_impl<A, true>(g, a, directed, from_cands);
-    return del_impl<A, true>(g, a, directed, from_cands);
-  }
-  if (what == 0) return build_impl<A, false>(g, a);
-  if (what == 1) return add_impl<A, false>(g, a, directed, from_cands);
-  return del_impl<A, false>(g, a, directed, from_cands);
+int dispatch_w(Graph &g, int what, uint64_t a, int directed, bool from_cands, int phase) {
+  if (g.weighted) return run_what<A, true>(g, what, a, directed, from_cands, phase);
+  return run_what<A, false>(g, what, a, directed, from_cands, phase);
 }
 
-int dispatch(Graph &g, int algo, int what, uint64_t a, int directed, bool from_cands) {
+// phase 0: enqueue the call's device work; phase 1: finish it after a sync.
+int dispatch(Graph &g, int algo, int what, uint64_t a, int directed, bool from_cands, int phase) {
   switch (algo) {
-    case RG_BFS: return dispatch_w<RG_BFS>(g, what, a, directed, from_cands);
-    case RG_SSSP: return dispatch_w<RG_SSSP>(g, what, a, directed, from_cands);
-    case RG_SSWP: return dispatch_w<RG_SSWP>(g, what, a, directed, from_cands);
-    case RG_WCC: return dispatch_w<RG_WCC>(g, what, a, directed, from_cands);
+    case RG_BFS: return dispatch_w<RG_BFS>(g, what, a, directed, from_cands, phase);
+    case RG_SSSP: return dispatch_w<RG_SSSP>(g, what, a, directed, from_cands, phase);
+    case RG_SSWP: return dispatch_w<RG_SSWP>(g, what, a, directed, from_cands, phase);
+    case RG_WCC: return dispatch_w<RG_WCC>(g, what, a, directed, from_cands, phase);
   }
   set_error("unknown algorithm");
   return RG_EINVAL;
@@ -987,6 +1544,8 @@ int tree_alloc(Graph &g) {
   };
   int rc;
   if ((rc = alloc((void **)&g.d.lab, V * 16 + 16, "labels"))) return rc;
+  if ((rc = alloc((void **)&g.d.val32, V * 4 + 4, "label value mirror"))) return rc;
+  RG_CUDA(cudaMemset(g.d.val32, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.d.stamp, V * 4 + 4, "frontier stamps"))) return rc;
   if ((rc = alloc((void **)&g.d.inv, V * 4 + 4, "invalidation tags"))) return rc;
   if ((rc = alloc((void **)&g.d.modstamp, V * 4 + 4, "modified stamps"))) return rc;
@@ -999,6 +1558,10 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.hubq, g.hubq_cap * 8, "hub tasks"))) return rc;
   if ((rc = alloc((void **)&g.lb_P, V * 8 + 16, "frontier degree prefix"))) return rc;
   if ((rc = alloc((void **)&g.act, V * 4 + 4, "dense-level activity"))) return rc;
+  if ((rc = alloc((void **)&g.lb_sums, SC_BLOCKS * 8, "scan block sums"))) return rc;
+  if ((rc = alloc((void **)&g.pull_P, V * 8 + 16, "in-degree prefix"))) return rc;
+  if ((rc = alloc((void **)&g.pull_base, V * 8 + 8, "in-segment bases"))) return rc;
+  if ((rc = alloc((void **)&g.pull_tile, (g.d.in.pool_cap / PL_TILE + 4) * 4, "pull partition"))) return rc;
   RG_CUDA(cudaMemset(g.act, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.lb_tile, (g.d.out.pool_cap / LB_TILE + 4) * 4, "tile partition"))) return rc;
   g.cub_tmp_bytes = 0;
@@ -1006,6 +1569,11 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc(&g.cub_tmp, g.cub_tmp_bytes + 256, "scan scratch"))) return rc;
   if ((rc = alloc((void **)&g.d.ctl, sizeof(unsigned long long) * C_COUNT, "control block"))) return rc;
   RG_CUDA(cudaMemset(g.d.ctl, 0, sizeof(unsigned long long) * C_COUNT));
+  {
+    unsigned long long one = 1;
+    RG_CUDA(cudaMemcpy(&g.d.ctl[C_MODEPOCH], &one, 8, cudaMemcpyHostToDevice));
+  }
+  if ((rc = alloc((void **)&g.d.trace, TRACE_CAP * 8, "level trace"))) return rc;
   RG_CUDA(cudaMemset(g.d.stamp, 0, V * 4 + 4));
   RG_CUDA(cudaMemset(g.d.inv, 0, V * 4 + 4));
   RG_CUDA(cudaMemset(g.d.modstamp, 0, V * 4 + 4));
@@ -1015,39 +1583,45 @@ int tree_alloc(Graph &g) {
   return RG_OK;
 }
 
-int tree_build(Graph &g, int algo, uint64_t root, uint64_t *total) {
+static void reset_stats(Graph &g) {
   g.st_levels = g.st_invalidated = g.st_recomputes = 0;
-  g.st_frontier.clear();
   g.st_level_ms.clear();
-  cudaMemsetAsync(&g.d.ctl[C_EDGES], 0, 8, g.stream);
-  g.algo = algo;
-  g.root = root;
-  int rc = dispatch(g, algo, 0, root, 1, false);
+}
+
+int tree_enqueue(Graph &g, int what, uint64_t n_edges, int directed, bool from_cands) {
+  reset_stats(g);
+  return dispatch(g, g.algo, what, n_edges, directed, from_cands, 0);
+}
+
+int tree_after_sync(Graph &g, int what, uint64_t *total) {
+  int rc = dispatch(g, g.algo, what, 0, 1, false, 1);
   if (rc) return rc;
   if (total) *total = g.h_ctl[C_RESULT];
   return RG_OK;
+}
+
+int tree_build(Graph &g, int algo, uint64_t root, uint64_t *total) {
+  reset_stats(g);
+  g.algo = algo;
+  g.root = root;
+  int rc = dispatch(g, algo, 0, root, 1, false, 0);
+  if (!rc) rc = read_ctl(g);
+  if (!rc) rc = tree_after_sync(g, 0, total);
+  return rc;
 }
 
 int tree_add(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total) {
-  g.st_levels = g.st_invalidated = g.st_recomputes = 0;
-  g.st_frontier.clear();
-  g.st_level_ms.clear();
-  cudaMemsetAsync(&g.d.ctl[C_EDGES], 0, 8, g.stream);
-  int rc = dispatch(g, g.algo, 1, n_edges, directed, from_cands);
-  if (rc) return rc;
-  if (total) *total = g.h_ctl[C_RESULT];
-  return RG_OK;
+  int rc = tree_enqueue(g, 1, n_edges, directed, from_cands);
+  if (!rc) rc = read_ctl(g);
+  if (!rc) rc = tree_after_sync(g, 1, total);
+  return rc;
 }
 
 int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t *total) {
-  g.st_levels = g.st_invalidated = g.st_recomputes = 0;
-  g.st_frontier.clear();
-  g.st_level_ms.clear();
-  cudaMemsetAsync(&g.d.ctl[C_EDGES], 0, 8, g.stream);
-  int rc = dispatch(g, g.algo, 2, n_edges, directed, from_cands);
-  if (rc) return rc;
-  if (total) *total = g.h_ctl[C_RESULT];
-  return RG_OK;
+  int rc = tree_enqueue(g, 2, n_edges, directed, from_cands);
+  if (!rc) rc = read_ctl(g);
+  if (!rc) rc = tree_after_sync(g, 2, total);
+  return rc;
 }
 
 int tree_classify(Graph &g, uint64_t n, int directed, const uint8_t *is_del_dev, uint8_t *unsafe_dev) {
