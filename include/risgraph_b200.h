@@ -200,6 +200,92 @@ int rg_build_tree_csr_static(int algo, uint64_t root, uint64_t vertices, uint64_
                              const uint64_t *row_offsets, const uint32_t *columns, const uint32_t *weights,
                              uint64_t *values, uint64_t *parents, void *cuda_stream);
 
+/* ---- Served mode ----------------------------------------------------------
+ * Stands in for the reference's latency-aware epoch loop of the _inc_rt
+ * drivers (src/sssp_inc_rt.cpp:119-441): clients submit single edge updates;
+ * the server batches, per graph instance, every update that arrived while the
+ * previous batch was on the GPU (continuous batching), applies it as one
+ * fused add batch + delete batch (safe updates cost only the multiplicity
+ * update; unsafe ones share one repair), and completes all of them together.
+ * Each instance has its own worker thread and CUDA stream, so instances of
+ * different sizes overlap on the device.  Instances are admitted against an
+ * HBM budget.  The epoch cap adapts so that one epoch stays within the target
+ * latency (the reference adapts its unsafe-update threshold at :394-412).
+ * With per_update = 1 every update is applied alone (one update per launch
+ * sequence): the baseline the batched server is measured against. */
+typedef struct rg_server rg_server;
+
+typedef struct {
+  uint32_t instance;  /* from rg_server_attach */
+  uint32_t type;      /* 0 = add edge, 1 = delete edge */
+  uint64_t src, dst, data;
+  uint64_t tag;       /* caller's id, returned in the completion */
+} rg_request;
+
+typedef struct {
+  uint64_t tag;
+  uint64_t submit_ns, done_ns;  /* CLOCK_MONOTONIC */
+  uint32_t instance, type;
+  int32_t status;               /* rg_status of the batch that applied it */
+  uint32_t epoch_size;
+} rg_completion;
+
+typedef struct {
+  uint64_t completed, epochs, largest_epoch;
+  double p50_us, p99_us, p999_us, max_us, mean_us;
+} rg_server_stats;
+
+int rg_server_create(uint64_t hbm_budget_bytes, double target_epoch_ms, uint64_t max_epoch, int per_update,
+                     rg_server **out);
+/* Admit a graph (labels already built with rg_build_tree for `algo`).
+ * RG_ENOMEM_HBM when its device bytes would exceed the budget. */
+int rg_server_attach(rg_server *s, rg_graph *g, int algo, int directed, uint32_t *instance);
+int rg_server_detach(rg_server *s, uint32_t instance);
+/* Thread-safe; timestamps the requests. */
+int rg_server_submit(rg_server *s, const rg_request *reqs, uint64_t n);
+/* Drain up to cap completions (n = number written). */
+int rg_server_poll(rg_server *s, rg_completion *out, uint64_t cap, uint64_t *n);
+/* Wait until every submitted request has completed (timeout_ms; RG_ETIMEOUT). */
+int rg_server_drain(rg_server *s, uint64_t timeout_ms);
+int rg_server_stats_get(rg_server *s, rg_server_stats *st, int reset);
+int rg_server_destroy(rg_server *s);
+
+/* Closed-loop client load (the reference's simulated clients, one outstanding
+ * update each, src/sssp_inc_rt.cpp:196-311), with exponential think time of
+ * mean think_us between a completion and the client's next update (Poisson
+ * arrivals per client).  Update number s (counted from `offset`, so that a
+ * load can continue the window of an earlier one) inserts pairs[imported + s/2]
+ * when s is even and deletes pairs[s/2] (the oldest loaded edge) when s is
+ * odd: the sliding window of src/sssp_inc.cpp:251-326.
+ * Weights as in rg_add_pairs when `weighted`.  The load stops issuing after
+ * duration_s seconds or max_updates updates (0 = no cap), or when the window
+ * reaches the end of `pairs`, and returns once all issued updates completed.
+ * Every delete removes a loaded copy, so the final graph, and hence the final
+ * values, depend only on the number of updates issued, not on their order. */
+typedef struct {
+  uint32_t instance;
+  uint32_t clients;
+  double think_us;
+  double duration_s;
+  uint64_t max_updates;
+  uint64_t offset;
+  const uint64_t *pairs;
+  uint64_t n_pairs, imported;
+  int weighted;
+  uint64_t seed;
+} rg_load_config;
+
+typedef struct {
+  uint64_t completed, adds, dels, failed;
+  double seconds, updates_per_s;
+  double p50_us, p99_us, p999_us, max_us, mean_us;
+  uint64_t epochs;        /* epochs of this instance during the load */
+  double mean_epoch;      /* updates per epoch */
+} rg_load_result;
+
+/* Runs the loads of n configs concurrently (one generator thread each). */
+int rg_server_run_load(rg_server *s, const rg_load_config *cfgs, uint64_t n, rg_load_result *results);
+
 const char *rg_status_string(int status);
 /* Last error message of the calling thread ("" if none). */
 const char *rg_last_error(void);

@@ -16,7 +16,8 @@ import re
 
 import numpy as np
 
-__all__ = ["Graph", "RGError", "EDGE_DTYPE", "ALGOS", "lib", "gen", "LIB_PATH"]
+__all__ = ["Graph", "Server", "RGError", "EDGE_DTYPE", "REQUEST_DTYPE", "COMPLETION_DTYPE", "ALGOS", "lib", "gen",
+           "LIB_PATH"]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "librisgraph_b200.so")
@@ -24,11 +25,37 @@ HEADER = os.path.join(os.path.dirname(PKG), "include", "risgraph_b200.h")
 
 ALGOS = {"bfs": 0, "sssp": 1, "sswp": 2, "wcc": 3}
 EDGE_DTYPE = np.dtype([("src", "<u8"), ("dst", "<u8"), ("data", "<u8")])  # rg_edge
+REQUEST_DTYPE = np.dtype([("instance", "<u4"), ("type", "<u4"), ("src", "<u8"), ("dst", "<u8"), ("data", "<u8"),
+                          ("tag", "<u8")])  # rg_request
+COMPLETION_DTYPE = np.dtype([("tag", "<u8"), ("submit_ns", "<u8"), ("done_ns", "<u8"), ("instance", "<u4"),
+                             ("type", "<u4"), ("status", "<i4"), ("epoch_size", "<u4")])  # rg_completion
 
 _u64 = ctypes.c_uint64
 _ptr = ctypes.c_void_p
 _int = ctypes.c_int
 _lib = None
+
+
+class ServerStats(ctypes.Structure):  # rg_server_stats
+    _fields_ = [("completed", ctypes.c_uint64), ("epochs", ctypes.c_uint64), ("largest_epoch", ctypes.c_uint64),
+                ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("p999_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double)]
+
+
+class LoadConfig(ctypes.Structure):  # rg_load_config
+    _fields_ = [("instance", ctypes.c_uint32), ("clients", ctypes.c_uint32), ("think_us", ctypes.c_double),
+                ("duration_s", ctypes.c_double), ("max_updates", ctypes.c_uint64), ("offset", ctypes.c_uint64),
+                ("pairs", ctypes.c_void_p),
+                ("n_pairs", ctypes.c_uint64), ("imported", ctypes.c_uint64), ("weighted", ctypes.c_int),
+                ("seed", ctypes.c_uint64)]
+
+
+class LoadResult(ctypes.Structure):  # rg_load_result
+    _fields_ = [("completed", ctypes.c_uint64), ("adds", ctypes.c_uint64), ("dels", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("seconds", ctypes.c_double), ("updates_per_s", ctypes.c_double),
+                ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("p999_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("epochs", ctypes.c_uint64),
+                ("mean_epoch", ctypes.c_double)]
 
 
 class RGError(RuntimeError):
@@ -74,6 +101,15 @@ def _declare(L):
         "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
         "rg_set_option": [P, _int, _u64],
         "rg_get_option": [P, _int, P],
+        "rg_server_create": [_u64, ctypes.c_double, _u64, _int, P],
+        "rg_server_attach": [P, P, _int, _int, P],
+        "rg_server_detach": [P, ctypes.c_uint32],
+        "rg_server_submit": [P, P, _u64],
+        "rg_server_poll": [P, P, _u64, P],
+        "rg_server_drain": [P, _u64],
+        "rg_server_stats_get": [P, P, _int],
+        "rg_server_run_load": [P, P, _u64, P],
+        "rg_server_destroy": [P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -364,3 +400,90 @@ class Graph:
 
 
 from . import gen  # noqa: E402  (synthetic inputs; needs lib())
+
+
+def _struct_dict(st) -> dict:
+    return {name: getattr(st, name) for name, _ in st._fields_}
+
+
+class Server:
+    """Served mode (rg_server_*): continuous batching of single-edge updates
+    over resident graph instances admitted against an HBM budget.
+
+    per_update=True applies every update alone (the plain one-update path).
+    While a graph is attached, only the server may touch it; detach (or
+    close) before calling the graph's own methods again.
+    """
+
+    def __init__(self, hbm_budget_bytes: int = 0, target_epoch_ms: float = 0.5, max_epoch: int = 65536,
+                 per_update: bool = False):
+        h = ctypes.c_void_p()
+        _check(lib().rg_server_create(int(hbm_budget_bytes), float(target_epoch_ms), int(max_epoch),
+                                      int(per_update), ctypes.byref(h)), "rg_server_create")
+        self._h = h
+        self._graphs = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rg_server_destroy(self._h)
+            self._h = None
+            self._graphs = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def attach(self, graph: Graph, directed: bool = True) -> int:
+        if graph.algo is None:
+            raise RuntimeError("build the graph's tree before attaching it")
+        inst = ctypes.c_uint32()
+        _check(lib().rg_server_attach(self._h, graph._h, ALGOS[graph.algo], int(directed), ctypes.byref(inst)),
+               "rg_server_attach")
+        self._graphs[inst.value] = graph
+        return inst.value
+
+    def detach(self, instance: int):
+        _check(lib().rg_server_detach(self._h, int(instance)), "rg_server_detach")
+        self._graphs.pop(int(instance), None)
+
+    def submit(self, requests):
+        r = np.ascontiguousarray(requests, dtype=REQUEST_DTYPE)
+        _check(lib().rg_server_submit(self._h, _p(r), len(r)), "rg_server_submit")
+
+    def poll(self, cap: int = 1 << 16) -> np.ndarray:
+        out = np.zeros(cap, dtype=COMPLETION_DTYPE)
+        n = _u64()
+        _check(lib().rg_server_poll(self._h, _p(out), cap, ctypes.byref(n)), "rg_server_poll")
+        return out[: n.value]
+
+    def drain(self, timeout_ms: int = 60000):
+        _check(lib().rg_server_drain(self._h, int(timeout_ms)), "rg_server_drain")
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        _check(lib().rg_server_stats_get(self._h, ctypes.byref(st), int(reset)), "rg_server_stats_get")
+        return _struct_dict(st)
+
+    def run_load(self, loads) -> list[dict]:
+        """loads: dicts with instance, clients, pairs (uint64 (n,2)), imported,
+        and optionally think_us, duration_s, max_updates, offset, weighted, seed."""
+        keep = []
+        cfgs = (LoadConfig * len(loads))()
+        for i, d in enumerate(loads):
+            pairs = np.ascontiguousarray(d["pairs"], dtype=np.uint64).reshape(-1, 2)
+            keep.append(pairs)
+            cfgs[i] = LoadConfig(int(d["instance"]), int(d["clients"]), float(d.get("think_us", 0.0)),
+                                 float(d.get("duration_s", 1.0)), int(d.get("max_updates", 0)),
+                                 int(d.get("offset", 0)), pairs.ctypes.data, len(pairs), int(d["imported"]), int(d.get("weighted", 0)),
+                                 int(d.get("seed", 1)))
+        res = (LoadResult * len(loads))()
+        _check(lib().rg_server_run_load(self._h, cfgs, len(loads), res), "rg_server_run_load")
+        return [_struct_dict(r) for r in res]

@@ -10,10 +10,6 @@
 
 #include "rg_internal.cuh"
 
-struct rg_graph {
-  rg::Graph g;
-};
-
 namespace rg {
 
 static thread_local std::string tl_err;

@@ -304,6 +304,9 @@ int storage_copy_old(Graph &g, uint64_t n_edges);
 const uint64_t *storage_old_host(Graph &g);
 int storage_error(Graph &g);
 int sync_ctl(Graph &g);
+// Size the staging and op buffers for batches of up to n_edges edges now, so
+// that later batches of that size allocate nothing.
+int storage_reserve(Graph &g, uint64_t n_edges);
 int storage_num(Graph &g, uint64_t nops, uint64_t *num);
 // op array accessors (device pointers)
 uint32_t *op_src(Graph &g);
@@ -328,3 +331,8 @@ int tree_checksum(Graph &g, uint64_t *sum);
 int tree_alloc(Graph &g);
 
 }  // namespace rg
+
+// The opaque handle of the C ABI.
+struct rg_graph {
+  rg::Graph g;
+};

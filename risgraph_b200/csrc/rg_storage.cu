@@ -404,6 +404,12 @@ int finish(Graph &g, bool need_old, uint64_t *old_num, uint64_t n) {
 
 }  // namespace
 
+int storage_reserve(Graph &g, uint64_t n_edges) {
+  int rc = ensure_ops(g, 2 * n_edges, n_edges);
+  if (!rc) rc = ensure_stage(g, n_edges * sizeof(rg_edge));
+  return rc;
+}
+
 uint32_t *op_src(Graph &g) { return g.ops + (uint64_t)O_SRC * g.ops_cap; }
 uint32_t *op_dst(Graph &g) { return g.ops + (uint64_t)O_DST * g.ops_cap; }
 uint32_t *op_w(Graph &g) { return g.ops + (uint64_t)O_W * g.ops_cap; }
