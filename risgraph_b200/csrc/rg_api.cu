@@ -77,6 +77,8 @@ int edge_updates(rg_graph *gh, const rg_edge *edges, const uint64_t *pairs, uint
   Graph &g = gh->g;
   int rc = check_edges(g, edges, pairs, n);
   if (rc) return rc;
+  // small batches (single updates, served epochs): one fused graph launch
+  if (apply && n && n <= rg::SMALL_EDGES && !g.profiling) return rg::apply_small(g, edges, pairs, n, directed, add, old_num);
   const int what = add ? 1 : 2;
   for (uint64_t b = 0; b < n; b += CHUNK_EDGES) {
     uint64_t m = std::min(CHUNK_EDGES, n - b), nops = 0;

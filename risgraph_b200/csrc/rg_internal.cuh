@@ -205,6 +205,19 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t *q, 
   if (pred) q[base + __popc(b & ((1u << lane_id()) - 1))] = v;
 }
 
+// Header of a small update batch in the graph's mapped pinned staging buffer,
+// read by the fused apply kernel; the edges follow at APPLY_DATA_OFF and the
+// per-edge old counts are written back at apply_old_off(cap).
+struct ApplyHdr {
+  uint64_t n;         // edges in the batch
+  uint64_t pairs;     // 1: reference-format (src,dst) pairs, 0: rg_edge records
+  uint64_t inv_tag;   // invalidation tag of a deletion repair
+  uint64_t want_old;  // 1: write the old counts back
+};
+constexpr uint64_t APPLY_DATA_OFF = 64;
+constexpr uint64_t SMALL_EDGES = 2048;  // largest batch of the fused single-CTA apply path
+inline uint64_t apply_old_off() { return APPLY_DATA_OFF + SMALL_EDGES * sizeof(rg_edge); }
+
 // A cached, instantiated level-loop graph.
 struct LoopGraph {
   cudaGraphExec_t exec = nullptr;
@@ -230,7 +243,8 @@ struct Graph {
   // staging for update batches
   void *stage_dev = nullptr;
   size_t stage_dev_bytes = 0;
-  void *stage_host = nullptr;  // pinned
+  void *stage_host = nullptr;  // pinned, mapped
+  void *stage_host_dev = nullptr;  // device view of stage_host
   size_t stage_host_bytes = 0;
   uint32_t *ops = nullptr;     // s,d,w,rid,old... per directed op (SoA inside)
   uint64_t ops_cap = 0;
@@ -254,6 +268,8 @@ struct Graph {
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
   LoopGraph loops[16];
   LoopGraph dels[8];
+  // fused small-batch apply graphs: [algo][weighted][add][directed]
+  LoopGraph applies[32];
   cudaStream_t cap_stream = nullptr;
   uint64_t layout_version = 1;  // bumped when pool buffers move (compaction)
   void *cub_tmp = nullptr;
@@ -329,6 +345,11 @@ int tree_classify(Graph &g, uint64_t n_edges, int directed, const uint8_t *is_de
 int tree_labels(Graph &g, uint64_t *val, uint64_t *par, uint64_t *pw);
 int tree_checksum(Graph &g, uint64_t *sum);
 int tree_alloc(Graph &g);
+// Fused small-batch apply (n <= SMALL_EDGES): storage update, candidate
+// selection and seeding in one single-CTA kernel, the repair loops behind a
+// conditional node, one graph launch and one synchronisation in all.
+int apply_small(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
+                uint64_t *old_num);
 
 }  // namespace rg
 

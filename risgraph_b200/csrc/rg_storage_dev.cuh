@@ -1,0 +1,271 @@
+// Device side of the edge storage (the B200 form of IndexedEdgeStorage,
+// core/storage.hpp:282-430, and Graph::add_edge / del_edge,
+// core/graph.hpp:203-253), as per-item functions.  rg_storage.cu wraps each
+// step in a grid-stride kernel for large batches; the fused small-batch apply
+// kernel of rg_tree.cu runs the same steps inside one CTA.
+#pragma once
+#include <type_traits>
+
+#include "rg_internal.cuh"
+
+namespace rg {
+namespace sdev {
+
+// Op arrays (u32 each, ops_cap entries) of a staged batch.  O_MUL: multiplicity
+// delta of the op (1; 2 for an undirected self-loop, whose two add_edge calls
+// hit the same key; 0 = no-op).
+enum OpArr { O_SRC = 0, O_DST, O_W, O_RID, O_OLD, O_MUL, O_SPARE, O_FLAG, O_NARR };
+
+struct OpView {
+  uint32_t *src, *dst, *w, *rid, *old, *mul, *spare, *flag;
+};
+
+inline OpView op_view(Graph &g) {
+  OpView v;
+  uint32_t **f = reinterpret_cast<uint32_t **>(&v);
+  for (int i = 0; i < O_NARR; i++) f[i] = g.ops + (uint64_t)i * g.ops_cap;
+  return v;
+}
+
+__device__ __forceinline__ uint64_t ht_hash(uint32_t s, uint32_t d, uint32_t w) {
+  return splitmix64(((uint64_t)s << 32 | d) ^ splitmix64((uint64_t)w + 0x5851F42D4C957F2Dull));
+}
+
+__device__ __forceinline__ void set_err(unsigned long long *ctl, int code) {
+  atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)code);
+}
+
+// Directed ops of edge i: one when directed; (s,d) and (d,s) when undirected
+// (add_edge(e,false), core/graph.hpp:206-211).  An undirected self-loop is a
+// single op of delta 2 on its one key, so concurrent duplicates still see a
+// serial sequence of counts.
+__device__ __forceinline__ void put_ops(OpView ops, uint64_t i, uint32_t s, uint32_t d, uint32_t w, int directed) {
+  if (directed) {
+    ops.src[i] = s; ops.dst[i] = d; ops.w[i] = w; ops.mul[i] = 1;
+  } else {
+    ops.src[2 * i] = s; ops.dst[2 * i] = d; ops.w[2 * i] = w; ops.mul[2 * i] = s == d ? 2 : 1;
+    ops.src[2 * i + 1] = d; ops.dst[2 * i + 1] = s; ops.w[2 * i + 1] = w; ops.mul[2 * i + 1] = s == d ? 0 : 1;
+  }
+}
+
+__device__ __forceinline__ void unpack_edge(const rg_edge *e, uint64_t i, int directed, int weighted, OpView ops) {
+  uint32_t s = (uint32_t)e[i].src, d = (uint32_t)e[i].dst, w = weighted ? (uint32_t)e[i].data : 0u;
+  put_ops(ops, i, s, d, w, directed);
+}
+
+// Reference file format pairs; weights are the pure function of the endpoints
+// used by every implementation here (splitmix64(src<<32|dst) % 255 + 1).
+__device__ __forceinline__ void unpack_pair(const uint64_t *p, uint64_t i, int directed, int weighted, OpView ops) {
+  uint64_t s64 = p[2 * i], d64 = p[2 * i + 1];
+  uint32_t s = (uint32_t)s64, d = (uint32_t)d64;
+  uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
+  put_ops(ops, i, s, d, w, directed);
+}
+
+// Find the record of op j's (s,d,w); create it (and reserve its slots at the
+// end of the src / dst segments) when `create`.  Vertices whose segment just
+// ran out of capacity go to the direction's grow list.
+__device__ __forceinline__ void lookup_op(const DevGraph &g, OpView ops, uint64_t j, int create) {
+  uint32_t s = ops.src[j], d = ops.dst[j], w = ops.w[j];
+  if (ops.mul[j] == 0) { ops.rid[j] = UNSET; ops.flag[j] = 0; return; }
+  ulonglong2 key = make_ulonglong2((uint64_t)s | ((uint64_t)d << 32), (uint64_t)w);
+  uint64_t h = ht_hash(s, d, w) & g.ht_mask;
+  uint32_t rid = UNSET, mine = UNSET;
+  int created = 0;
+  for (uint64_t probe = 0; probe <= g.ht_mask; probe++) {
+    ulonglong2 e = __ldcg(&g.ht[h]);
+    if ((uint32_t)e.x == NONE) {
+      if (!create) break;
+      if (mine == UNSET) {
+        unsigned long long r = atomicAdd(g.rec_top, 1ull);
+        if (r >= g.rec_cap) { set_err(g.ctl, RG_ENOSPACE); break; }
+        mine = (uint32_t)r;
+        g.rec_num[mine] = 0;
+        g.rec_out[mine] = UNSET;
+        g.rec_in[mine] = UNSET;
+        __threadfence();
+      }
+      ulonglong2 want = make_ulonglong2(key.x, key.y | ((uint64_t)mine << 32));
+      ulonglong2 old = cas128(&g.ht[h], make_ulonglong2(~0ull, ~0ull), want);
+      if (old.x == ~0ull && old.y == ~0ull) { rid = mine; created = 1; break; }
+      e = old;
+    }
+    // A 16-byte load racing with the claiming CAS may see the new (src,dst)
+    // half with the old (all-ones) half; re-read atomically before deciding.
+    if (e.x == key.x && (uint32_t)e.y != w) e = cas128(&g.ht[h], make_ulonglong2(~0ull, ~0ull), make_ulonglong2(~0ull, ~0ull));
+    if (e.x == key.x && (uint32_t)e.y == w) { rid = (uint32_t)(e.y >> 32); break; }
+    h = (h + 1) & g.ht_mask;
+  }
+  if (create && rid == UNSET && mine == UNSET) set_err(g.ctl, RG_ENOSPACE);
+  ops.rid[j] = rid;
+  ops.flag[j] = created;
+  if (created) {
+    uint32_t po = atomicAdd(&g.out.len[s], 1u);
+    g.rec_out[rid] = po;
+    if (po == g.out.cap[s]) {
+      unsigned long long k = atomicAdd(&g.ctl[C_GROWN_OUT], 1ull);
+      g.out.grow[k] = s;
+    }
+    if (!g.symmetric) {
+      uint32_t pi = atomicAdd(&g.in.len[d], 1u);
+      g.rec_in[rid] = pi;
+      if (pi == g.in.cap[d]) {
+        unsigned long long k = atomicAdd(&g.ctl[C_GROWN_IN], 1ull);
+        g.in.grow[k] = d;
+      }
+    }
+  }
+}
+
+// Grow vertex v of a direction, cooperatively by the calling CTA: a new region
+// from the pool bump pointer, then a copy of the existing slots.  Initial loads
+// (cap 0) get exactly len + len/8 + 2; a full pool sets RG_ENOSPACE with
+// C_AUX = 1 (the host compacts and replays).  All threads of the CTA call it.
+struct GrowShared {
+  uint64_t new_off;
+  uint32_t copy, new_cap;
+};
+
+template <bool W>
+__device__ __forceinline__ void grow_vertex(DevDir dir, unsigned long long *ctl, uint32_t v, GrowShared &sh) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *pool = reinterpret_cast<E *>(dir.pool);
+  if (threadIdx.x == 0) {
+    uint32_t len = dir.len[v], cap = dir.cap[v];
+    sh.new_cap = 0;
+    if (len > cap) {  // (a retry after compaction skips vertices already grown)
+      uint64_t want = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
+      while (want < len) want *= 2;
+      if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
+      unsigned long long off = atomicAdd(dir.pool_top, (unsigned long long)want);
+      if (off + want > dir.pool_cap) {
+        atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
+        ctl[C_AUX] = 1;
+      } else {
+        sh.new_cap = (uint32_t)want;
+        sh.new_off = off;
+      }
+    }
+    sh.copy = len < cap ? len : cap;
+  }
+  __syncthreads();
+  if (sh.new_cap) {
+    uint64_t from = dir.off[v];
+    uint32_t old_cap = dir.cap[v];
+    for (uint32_t i = threadIdx.x; i < sh.copy; i += blockDim.x) {
+      pool[sh.new_off + i] = pool[from + i];
+      dir.owner[sh.new_off + i] = v;
+    }
+    for (uint32_t i = threadIdx.x; i < old_cap; i += blockDim.x) dir.owner[from + i] = NONE;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      dir.off[v] = sh.new_off;
+      dir.cap[v] = sh.new_cap;
+    }
+  }
+  __syncthreads();
+}
+
+// Store op j's new entries (created by lookup), still DEAD (multiplicity 0).
+template <bool W>
+__device__ __forceinline__ void write_new_op(const DevGraph &g, OpView ops, uint64_t j) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *po = reinterpret_cast<E *>(g.out.pool);
+  E *pi = reinterpret_cast<E *>(g.in.pool);
+  if (!ops.flag[j]) return;
+  uint32_t s = ops.src[j], d = ops.dst[j], w = ops.w[j], rid = ops.rid[j];
+  uint32_t ps = g.rec_out[rid];
+  if (ps < g.out.cap[s]) {
+    if constexpr (W) po[g.out.off[s] + ps] = make_uint2(d | DEAD, w);
+    else po[g.out.off[s] + ps] = d | DEAD;
+    g.out.owner[g.out.off[s] + ps] = s;
+  }
+  if (!g.symmetric) {
+    uint32_t pd = g.rec_in[rid];
+    if (pd < g.in.cap[d]) {
+      if constexpr (W) pi[g.in.off[d] + pd] = make_uint2(s | DEAD, w);
+      else pi[g.in.off[d] + pd] = s | DEAD;
+      g.in.owner[g.in.off[d] + pd] = d;
+    }
+  }
+}
+
+template <bool W>
+__device__ __forceinline__ void set_alive(const DevDir &dir, uint32_t v, uint32_t pos, uint32_t nbr, bool alive) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *pool = reinterpret_cast<E *>(dir.pool);
+  if (pos >= dir.cap[v]) return;
+  uint32_t x = alive ? nbr : (nbr | DEAD);
+  if constexpr (W) reinterpret_cast<uint32_t *>(&pool[dir.off[v] + pos])[0] = x;
+  else pool[dir.off[v] + pos] = x;
+}
+
+// Multiplicity update of op j (update_edge, core/storage.hpp:390-396); the
+// 0->1 and 1->0 transitions flip the DEAD bit.  ops.old = count before.
+template <bool W>
+__device__ __forceinline__ void count_op(const DevGraph &g, OpView ops, uint64_t j, int add) {
+  uint32_t rid = ops.rid[j];
+  uint32_t s = ops.src[j], d = ops.dst[j];
+  if (rid == UNSET) { ops.old[j] = 0; return; }
+  const uint32_t mul = ops.mul[j];
+  uint32_t old;
+  if (add) {
+    old = atomicAdd(&g.rec_num[rid], mul);
+    atomicAdd(&g.out.deg[s], (unsigned long long)mul);
+    if (!g.symmetric) atomicAdd(&g.in.deg[d], (unsigned long long)mul);
+    if (old == 0) {
+      set_alive<W>(g.out, s, g.rec_out[rid], d, true);
+      if (!g.symmetric) set_alive<W>(g.in, d, g.rec_in[rid], s, true);
+    }
+  } else {
+    // update_edge(-1): the count never goes below zero
+    old = g.rec_num[rid];
+    while (old > 0) {
+      uint32_t nv = old >= mul ? old - mul : 0u;
+      uint32_t seen = atomicCAS(&g.rec_num[rid], old, nv);
+      if (seen == old) break;
+      old = seen;
+    }
+    uint32_t dropped = old < mul ? old : mul;
+    if (dropped) {
+      atomicAdd(&g.out.deg[s], 0ull - dropped);
+      if (!g.symmetric) atomicAdd(&g.in.deg[d], 0ull - dropped);
+    }
+    if (old != 0 && old <= mul) {
+      set_alive<W>(g.out, s, g.rec_out[rid], d, false);
+      if (!g.symmetric) set_alive<W>(g.in, d, g.rec_in[rid], s, false);
+    }
+  }
+  ops.old[j] = old;
+}
+
+// Per-edge old multiplicity with add_edge/del_edge's undirected conventions
+// (core/graph.hpp:206-211: second orientation's count, minus one for a
+// self-loop on add; :232-237 for delete) and the tree-repair candidates:
+// 0->1 adds (src/sssp_inc_batch.cpp:148) and 1->0 deletes (:166).
+__device__ __forceinline__ void edge_old(OpView ops, uint64_t i, int directed, int add, int collect,
+                                         uint64_t *old_out, uint32_t *cand, unsigned long long *ctl) {
+  uint32_t o;
+  if (directed) {
+    o = ops.old[i];
+  } else {
+    const uint32_t s = ops.src[2 * i], d = ops.dst[2 * i];
+    if (s == d) {
+      // add returns old+1-1, delete the second call's old (max(old-1,0))
+      uint32_t a = ops.old[2 * i];
+      o = add ? a : (a ? a - 1 : 0);
+    } else {
+      // both orientations move together; the canonical (lower src) key gives a
+      // serial count sequence even when (s,d) and (d,s) share a batch
+      o = ops.old[2 * i + (s < d ? 0 : 1)];
+    }
+  }
+  if (old_out) old_out[i] = o;
+  if (collect && (add ? o == 0 : o == 1)) {
+    unsigned long long k = atomicAdd(&ctl[C_CANDN], 1ull);
+    cand[k] = (uint32_t)i;
+  }
+}
+
+}  // namespace sdev
+}  // namespace rg

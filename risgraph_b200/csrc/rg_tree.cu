@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
 
 #include <cub/block/block_reduce.cuh>
@@ -26,6 +27,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "rg_internal.cuh"
+#include "rg_storage_dev.cuh"
 
 namespace rg {
 
@@ -727,8 +729,7 @@ __global__ void k_bfs_bottom_up(DevGraph g, uint32_t *fout, unsigned long long *
 // host round trip happens between levels (the reference's driver decides
 // between levels on the host, core/graph.hpp:898-983, :1013-1111).
 
-__global__ void k_prologue(DevGraph g, unsigned long long inv_tag) {
-  unsigned long long *c = g.ctl;
+__device__ __forceinline__ void prologue_ctl(unsigned long long *c, unsigned long long inv_tag) {
   c[C_INVTAG] = inv_tag;
   c[C_INVITER] = 0;
   c[C_QN0] = 0;
@@ -743,6 +744,8 @@ __global__ void k_prologue(DevGraph g, unsigned long long inv_tag) {
   c[C_KLAUNCH] = 0;
   c[C_STAMP] += 1;
 }
+
+__global__ void k_prologue(DevGraph g, unsigned long long inv_tag) { prologue_ctl(g.ctl, inv_tag); }
 
 // Kernels a level of each mode launches (k_level_begin not included).
 __host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
@@ -856,13 +859,11 @@ __global__ void k_init(DevGraph g, uint64_t root, uint32_t *fout) {
 // Seed relaxations of update_tree_add (single :1140-1153, batch :1180-1214):
 // relax each inserted edge, both orientations when undirected.
 template <int A>
-__global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, const uint32_t *ow, const uint32_t *cand,
-                           const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t *fout,
-                           unsigned long long *fout_n, uint32_t mst) {
+__device__ __forceinline__ unsigned long long seed_add(const DevGraph &g, const uint32_t *os, const uint32_t *od,
+                                                       const uint32_t *ow, const uint32_t *cand, uint64_t n,
+                                                       int directed, uint32_t *fout, unsigned long long *fout_n,
+                                                       uint32_t mst, uint64_t warp, uint64_t nwarps) {
   const uint32_t st = (uint32_t)g.ctl[C_STAMP];
-  const uint64_t n = cand ? *cand_n : n_all;
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long local = 0;
   for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
     uint64_t i = base + lane_id();
@@ -874,7 +875,7 @@ __global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, c
         uint64_t op = directed ? e : 2 * e + dir;
         uint32_t u = os[op];
         v = od[op];
-        upd = relax<A>(g,u, ld_v32(g.val32, u), v, ow[op]);
+        upd = relax<A>(g, u, ld_v32(g.val32, u), v, ow[op]);
       }
       local += upd;
       bool app = upd && atomicExch(&g.stamp[v], st) != st;
@@ -882,18 +883,26 @@ __global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, c
       if (mst) mark_modified(g, upd, v, mst);
     }
   }
+  return local;
+}
+
+template <int A>
+__global__ void k_seed_add(DevGraph g, const uint32_t *os, const uint32_t *od, const uint32_t *ow, const uint32_t *cand,
+                           const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t *fout,
+                           unsigned long long *fout_n, uint32_t mst) {
+  const uint64_t n = cand ? *cand_n : n_all;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long local = seed_add<A>(g, os, od, ow, cand, n, directed, fout, fout_n, mst, warp, nwarps);
   warp_add_result(local, &g.ctl[C_RESULT]);
 }
 
 // Seeds of update_tree_del (single :1640-1649, batch :1680-1714): a deleted
 // edge that is dst's parent edge invalidates dst.
-__global__ void k_seed_del(DevGraph g, const uint32_t *os, const uint32_t *od, const uint32_t *ow, const uint32_t *cand,
-                           const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t *fout,
-                           unsigned long long *fout_n) {
+__device__ __forceinline__ void seed_del(const DevGraph &g, const uint32_t *os, const uint32_t *od, const uint32_t *ow,
+                                         const uint32_t *cand, uint64_t n, int directed, uint32_t *fout,
+                                         unsigned long long *fout_n, uint64_t warp, uint64_t nwarps) {
   const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
-  const uint64_t n = cand ? *cand_n : n_all;
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
     uint64_t i = base + lane_id();
     for (int dir = 0; dir < (directed ? 1 : 2); dir++) {
@@ -909,6 +918,98 @@ __global__ void k_seed_del(DevGraph g, const uint32_t *os, const uint32_t *od, c
       warp_append(app, v, fout, fout_n, FULL);
     }
   }
+}
+
+__global__ void k_seed_del(DevGraph g, const uint32_t *os, const uint32_t *od, const uint32_t *ow, const uint32_t *cand,
+                           const unsigned long long *cand_n, uint64_t n_all, int directed, uint32_t *fout,
+                           unsigned long long *fout_n) {
+  const uint64_t n = cand ? *cand_n : n_all;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  seed_del(g, os, od, ow, cand, n, directed, fout, fout_n, warp, nwarps);
+}
+
+// Fused small-batch apply: one CTA runs the storage steps of a batch of at
+// most SMALL_EDGES edges (unpack from the mapped staging buffer, lookup/create,
+// growth, new-slot write, multiplicity count, candidates) and the seeding of
+// the tree repair, with CTA barriers where the multi-kernel path has kernel
+// boundaries.  It then opens the conditional node that runs the repair loops
+// only when the seeds produced a frontier: a safe update (the common case,
+// need_update_tree_* false) costs this one kernel.  A storage error (edge index
+// or pool full) stops before the count step, leaving the op arrays for the
+// host's compaction and replay, exactly like the multi-kernel path.
+constexpr int FS_TPB = 1024;
+
+template <int A, bool W>
+__global__ void __launch_bounds__(FS_TPB)
+    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const void *data, uint64_t *old_host,
+                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, cudaGraphConditionalHandle repair) {
+  __shared__ sdev::GrowShared gsh;
+  __shared__ uint64_t s_n, s_pairs, s_want;
+  unsigned long long *c = g.ctl;
+  const unsigned tid = threadIdx.x;
+  if (tid == 0) {
+    // the host wrote the header before the launch; read it past any cache
+    s_n = __ldcv(&hdr->n);
+    s_pairs = __ldcv(&hdr->pairs);
+    s_want = __ldcv(&hdr->want_old);
+    prologue_ctl(c, __ldcv(&hdr->inv_tag));
+    c[C_CANDN] = 0;
+    c[C_GROWN_OUT] = 0;
+    c[C_GROWN_IN] = 0;
+  }
+  __syncthreads();
+  const uint64_t n = s_n < SMALL_EDGES ? s_n : SMALL_EDGES;
+  const uint64_t nops = directed ? n : 2 * n;
+  const int weighted = W ? 1 : 0;
+  if (s_pairs) {
+    const uint64_t *p = reinterpret_cast<const uint64_t *>(data);
+    for (uint64_t i = tid; i < n; i += FS_TPB) {
+      uint64_t s64 = __ldcv(&p[2 * i]), d64 = __ldcv(&p[2 * i + 1]);
+      uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
+      sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, w, directed);
+    }
+  } else {
+    const uint64_t *e = reinterpret_cast<const uint64_t *>(data);
+    for (uint64_t i = tid; i < n; i += FS_TPB) {
+      uint64_t s64 = __ldcv(&e[3 * i]), d64 = __ldcv(&e[3 * i + 1]), w64 = __ldcv(&e[3 * i + 2]);
+      sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, weighted ? (uint32_t)w64 : 0u, directed);
+    }
+  }
+  __syncthreads();
+  for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::lookup_op(g, ops, j, add);
+  __syncthreads();
+  if (add) {
+    const unsigned long long no = c[C_GROWN_OUT];
+    for (unsigned long long k = 0; k < no; k++) sdev::grow_vertex<W>(g.out, c, g.out.grow[k], gsh);
+    if (!g.symmetric) {
+      const unsigned long long ni = c[C_GROWN_IN];
+      for (unsigned long long k = 0; k < ni; k++) sdev::grow_vertex<W>(g.in, c, g.in.grow[k], gsh);
+    }
+  }
+  __syncthreads();
+  if (c[C_ERR]) {
+    if (tid == 0) cudaGraphSetConditional(repair, 0u);
+    return;
+  }
+  if (add) {
+    for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::write_new_op<W>(g, ops, j);
+    __syncthreads();
+  }
+  for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::count_op<W>(g, ops, j, add);
+  __syncthreads();
+  for (uint64_t i = tid; i < n; i += FS_TPB) sdev::edge_old(ops, i, directed, add, 1, s_want ? old_host : nullptr, cand, c);
+  __syncthreads();
+  const uint64_t ncand = c[C_CANDN];
+  const uint64_t warp = tid >> 5, nwarps = FS_TPB / 32;
+  if (add) {
+    unsigned long long local = seed_add<A>(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], mst, warp, nwarps);
+    warp_add_result(local, &c[C_RESULT]);
+  } else {
+    seed_del(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], warp, nwarps);
+  }
+  __syncthreads();
+  if (tid == 0) cudaGraphSetConditional(repair, (c[C_QN0] && !c[C_ERR]) ? 1u : 0u);
 }
 
 // has_parents (core/graph.hpp:1889-1907): does x's parent chain reach a root
@@ -1215,31 +1316,21 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   return cfg;
 }
 
-// The level loop as a CUDA graph:
+uint64_t recompute_threshold(const Graph &g) {
+  return std::max<uint64_t>((uint64_t)(0.05 * (double)g.V), g.recompute_min);
+}
+
+// The level loop as a node of a CUDA graph:
 //   WHILE (frontier non-empty) {
 //     k_level_begin(q0 -> q1) ; SWITCH(mode) { sparse | pull | dense push | bottom-up | edge-balanced }
 //     k_level_begin(q1 -> q0) ; SWITCH(mode) { ... }
 //     k_loop_cond
 //   }
-// Built once per (algorithm, weighting, variant) and cached until the pool is
-// relocated by a compaction or an option changes.
+// added to `graph` after `deps`.
 template <int A, bool W>
-int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
-  const LevelCfg cfg = level_cfg(g, A, build_variant);
-  LoopGraph &slot = g.loops[(A * 2 + (W ? 1 : 0)) * 2 + (build_variant ? 1 : 0)];
-  const uint64_t key = (g.layout_version << 40) ^ (cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^
-                       ((uint64_t)cfg.allow_pull << 1) ^ (uint64_t)cfg.bottom_up;
-  if (slot.exec && slot.key == key) {
-    *out = slot.exec;
-    return RG_OK;
-  }
-  if (slot.exec) {
-    cudaGraphExecDestroy(slot.exec);
-    slot.exec = nullptr;
-  }
+int add_level_loop(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps, const LevelCfg &cfg,
+                   cudaGraphNode_t *out) {
   if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
-  cudaGraph_t graph;
-  RG_CUDA(cudaGraphCreate(&graph, 0));
   int rc = RG_OK;
   cudaError_t e = cudaSuccess;
   do {
@@ -1250,8 +1341,7 @@ int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
     wp.conditional.handle = wh;
     wp.conditional.type = cudaGraphCondTypeWhile;
     wp.conditional.size = 1;
-    cudaGraphNode_t wnode;
-    if ((e = cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp)) != cudaSuccess) break;
+    if ((e = cudaGraphAddNode(out, graph, deps, ndeps, &wp)) != cudaSuccess) break;
     cudaGraph_t body = wp.conditional.phGraph_out[0];
     cudaGraphNode_t prev = nullptr;
     for (int half = 0; half < 2 && e == cudaSuccess && !rc; half++) {
@@ -1298,14 +1388,101 @@ int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
     cp.blockDim = dim3(1);
     cp.kernelParams = cargs;
     cudaGraphNode_t cn;
-    if ((e = cudaGraphAddKernelNode(&cn, body, &prev, 1, &cp)) != cudaSuccess) break;
-    e = cudaGraphInstantiate(&slot.exec, graph, 0);
+    e = cudaGraphAddKernelNode(&cn, body, &prev, 1, &cp);
   } while (0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
-    slot.exec = nullptr;
-    return cuda_fail(e, "building the level-loop graph");
+  if (e != cudaSuccess) return cuda_fail(e, "building the level-loop graph");
+  return rc;
+}
+
+// Deletion repair as nodes of a CUDA graph (do_update_tree_del,
+// core/graph.hpp:1235-1612):
+//   WHILE (invalidated frontier non-empty and no recompute) {
+//     k_inv_begin ; k_rescue ; k_expand     (queue 0 -> 1)
+//     k_inv_begin ; k_rescue ; k_expand     (queue 1 -> 0)
+//     k_inv_cond }
+//   k_reset ; k_pull ; k_copy_frontier (reset set -> queue 0 for the push loop)
+template <int A, bool W>
+int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps, cudaGraphNode_t *out) {
+  if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
+  const uint64_t big = recompute_threshold(g);
+  const uint64_t limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
+  uint32_t mst = mod_stamp(g);
+  const int gridw = g.num_sms * 16;
+  cudaError_t e = cudaSuccess;
+  do {
+    cudaGraphConditionalHandle wh;
+    if ((e = cudaGraphConditionalHandleCreate(&wh, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = wh;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    if ((e = cudaGraphAddNode(&wnode, graph, deps, ndeps, &wp)) != cudaSuccess) break;
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+        cudaSuccess)
+      break;
+    for (int half = 0; half < 2; half++) {
+      unsigned long long *fin_n = &g.d.ctl[C_QN0 + half], *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
+      k_inv_begin<<<1, 1, 0, g.cap_stream>>>(g.d, fin_n, fout_n, big);
+      k_rescue<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, limit);
+      k_expand<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
+    }
+    k_inv_cond<<<1, 1, 0, g.cap_stream>>>(g.d, &g.d.ctl[C_QN0], (uint64_t)g.V + 2, wh);
+    if ((e = cudaStreamEndCapture(g.cap_stream, &body)) != cudaSuccess) break;
+    // k_reset -> k_pull -> k_copy_frontier after the loop
+    unsigned long long *tree_n = &g.d.ctl[C_TREEN], *q0_n = &g.d.ctl[C_QN0];
+    uint32_t *q0 = g.q[0];
+    const uint32_t *tree = g.tree;
+    void *ra[] = {(void *)&g.d, (void *)&tree, (void *)&tree_n, (void *)&mst};
+    void *ca[] = {(void *)&g.d, (void *)&tree, (void *)&tree_n, (void *)&q0, (void *)&q0_n};
+    cudaKernelNodeParams kp = {};
+    kp.gridDim = dim3(gridw);
+    kp.blockDim = dim3(TPB);
+    kp.func = (void *)k_reset<A>;
+    kp.kernelParams = ra;
+    cudaGraphNode_t n1, n2;
+    if ((e = cudaGraphAddKernelNode(&n1, graph, &wnode, 1, &kp)) != cudaSuccess) break;
+    kp.func = (void *)k_pull<A, W>;
+    if ((e = cudaGraphAddKernelNode(&n2, graph, &n1, 1, &kp)) != cudaSuccess) break;
+    kp.func = (void *)k_copy_frontier;
+    kp.gridDim = dim3(g.num_sms * 4);
+    kp.kernelParams = ca;
+    e = cudaGraphAddKernelNode(out, graph, &n2, 1, &kp);
+  } while (0);
+  if (e != cudaSuccess) return cuda_fail(e, "building the deletion-repair graph");
+  return RG_OK;
+}
+
+// Cached standalone level loop per (algorithm, weighting, variant), rebuilt
+// when the pool is relocated by a compaction or an option changes.
+template <int A, bool W>
+int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
+  const LevelCfg cfg = level_cfg(g, A, build_variant);
+  LoopGraph &slot = g.loops[(A * 2 + (W ? 1 : 0)) * 2 + (build_variant ? 1 : 0)];
+  const uint64_t key = (g.layout_version << 40) ^ (cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^
+                       ((uint64_t)cfg.allow_pull << 1) ^ (uint64_t)cfg.bottom_up;
+  if (slot.exec && slot.key == key) {
+    *out = slot.exec;
+    return RG_OK;
   }
+  if (slot.exec) {
+    cudaGraphExecDestroy(slot.exec);
+    slot.exec = nullptr;
+  }
+  cudaGraph_t graph;
+  RG_CUDA(cudaGraphCreate(&graph, 0));
+  cudaGraphNode_t node;
+  int rc = add_level_loop<A, W>(g, graph, nullptr, 0, cfg, &node);
+  if (!rc) {
+    cudaError_t e = cudaGraphInstantiate(&slot.exec, graph, 0);
+    if (e != cudaSuccess) {
+      slot.exec = nullptr;
+      rc = cuda_fail(e, "instantiating the level-loop graph");
+    }
+  }
+  cudaGraphDestroy(graph);
   if (rc) return rc;
   slot.key = key;
   *out = slot.exec;
@@ -1356,21 +1533,12 @@ int push_levels(Graph &g, bool build_variant) {
   return RG_OK;
 }
 
-uint64_t recompute_threshold(const Graph &g) {
-  return std::max<uint64_t>((uint64_t)(0.05 * (double)g.V), g.recompute_min);
-}
 
-// Deletion repair as a graph (do_update_tree_del, core/graph.hpp:1235-1612):
-//   WHILE (invalidated frontier non-empty and no recompute) {
-//     k_inv_begin ; k_rescue ; k_expand     (queue 0 -> 1)
-//     k_inv_begin ; k_rescue ; k_expand     (queue 1 -> 0)
-//     k_inv_cond }
-//   k_reset ; k_pull ; k_copy_frontier (reset set -> queue 0 for the push loop)
+// Cached standalone deletion repair (the push loop follows as its own graph).
 template <int A, bool W>
 int del_exec(Graph &g, cudaGraphExec_t *out) {
   LoopGraph &slot = g.dels[A * 2 + (W ? 1 : 0)];
-  const uint64_t big = recompute_threshold(g);
-  const uint64_t key = (g.layout_version << 40) ^ big;
+  const uint64_t key = (g.layout_version << 40) ^ recompute_threshold(g);
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
     return RG_OK;
@@ -1379,52 +1547,19 @@ int del_exec(Graph &g, cudaGraphExec_t *out) {
     cudaGraphExecDestroy(slot.exec);
     slot.exec = nullptr;
   }
-  if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
-  const uint64_t limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
-  const uint32_t mst = mod_stamp(g);
-  const int gridw = g.num_sms * 16;
   cudaGraph_t graph;
   RG_CUDA(cudaGraphCreate(&graph, 0));
-  cudaError_t e = cudaSuccess;
-  do {
-    cudaGraphConditionalHandle wh;
-    if ((e = cudaGraphConditionalHandleCreate(&wh, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    cudaGraphNodeParams wp = {};
-    wp.type = cudaGraphNodeTypeConditional;
-    wp.conditional.handle = wh;
-    wp.conditional.type = cudaGraphCondTypeWhile;
-    wp.conditional.size = 1;
-    cudaGraphNode_t wnode;
-    if ((e = cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp)) != cudaSuccess) break;
-    cudaGraph_t body = wp.conditional.phGraph_out[0];
-    if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
-        cudaSuccess)
-      break;
-    for (int half = 0; half < 2; half++) {
-      unsigned long long *fin_n = &g.d.ctl[C_QN0 + half], *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
-      k_inv_begin<<<1, 1, 0, g.cap_stream>>>(g.d, fin_n, fout_n, big);
-      k_rescue<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, limit);
-      k_expand<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
+  cudaGraphNode_t last;
+  int rc = add_del_repair<A, W>(g, graph, nullptr, 0, &last);
+  if (!rc) {
+    cudaError_t e = cudaGraphInstantiate(&slot.exec, graph, 0);
+    if (e != cudaSuccess) {
+      slot.exec = nullptr;
+      rc = cuda_fail(e, "instantiating the deletion-repair graph");
     }
-    k_inv_cond<<<1, 1, 0, g.cap_stream>>>(g.d, &g.d.ctl[C_QN0], (uint64_t)g.V + 2, wh);
-    e = cudaStreamEndCapture(g.cap_stream, &body);
-    if (e != cudaSuccess) break;
-    if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, graph, &wnode, nullptr, 1, cudaStreamCaptureModeRelaxed)) !=
-        cudaSuccess)
-      break;
-    k_reset<A><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
-    k_pull<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
-    k_copy_frontier<<<g.num_sms * 4, TPB, 0, g.cap_stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], g.q[0], &g.d.ctl[C_QN0]);
-    cudaGraph_t g2 = graph;
-    e = cudaStreamEndCapture(g.cap_stream, &g2);
-    if (e != cudaSuccess) break;
-    e = cudaGraphInstantiate(&slot.exec, graph, 0);
-  } while (0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
-    slot.exec = nullptr;
-    return cuda_fail(e, "building the deletion-repair graph");
   }
+  cudaGraphDestroy(graph);
+  if (rc) return rc;
   slot.key = key;
   *out = slot.exec;
   return RG_OK;
@@ -1622,6 +1757,152 @@ int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t
   if (!rc) rc = read_ctl(g);
   if (!rc) rc = tree_after_sync(g, 2, total);
   return rc;
+}
+
+// Fused small-batch apply graph per (algorithm, weighting, add/delete,
+// directed): k_apply_small -> IF (frontier) { [deletion repair ->] level loop }
+// -> control block to the host.  Its parameters hold the op, staging and pool
+// addresses, so it is rebuilt when any of them moves.
+template <int A, bool W>
+int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
+  LoopGraph &slot = g.applies[((A * 2 + (W ? 1 : 0)) * 2 + (add ? 1 : 0)) * 2 + (directed ? 1 : 0)];
+  const LevelCfg cfg = level_cfg(g, A, false);
+  const uint64_t key = splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
+                       splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^
+                       splitmix64((cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^ 3) ^
+                       splitmix64(recompute_threshold(g) + 11);
+  if (slot.exec && slot.key == key) {
+    *out = slot.exec;
+    return RG_OK;
+  }
+  if (slot.exec) {
+    cudaGraphExecDestroy(slot.exec);
+    slot.exec = nullptr;
+  }
+  cudaGraph_t graph;
+  RG_CUDA(cudaGraphCreate(&graph, 0));
+  int rc = RG_OK;
+  cudaError_t e = cudaSuccess;
+  do {
+    cudaGraphConditionalHandle ih;
+    if ((e = cudaGraphConditionalHandleCreate(&ih, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    sdev::OpView ops = sdev::op_view(g);
+    char *base = reinterpret_cast<char *>(g.stage_host_dev);
+    const ApplyHdr *hdr = reinterpret_cast<const ApplyHdr *>(base);
+    const void *data = base + APPLY_DATA_OFF;
+    uint64_t *old_host = reinterpret_cast<uint64_t *>(base + apply_old_off());
+    uint32_t *cand = op_cand(g);
+    int a_add = add ? 1 : 0, a_dir = directed ? 1 : 0;
+    uint32_t *q0 = g.q[0];
+    uint32_t mst = mod_stamp(g);
+    void *args[] = {(void *)&g.d, (void *)&ops, (void *)&hdr, (void *)&data, (void *)&old_host, (void *)&cand,
+                    (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&ih};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *)k_apply_small<A, W>;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(FS_TPB);
+    kp.kernelParams = args;
+    cudaGraphNode_t kn;
+    if ((e = cudaGraphAddKernelNode(&kn, graph, nullptr, 0, &kp)) != cudaSuccess) break;
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = ih;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t ifn;
+    if ((e = cudaGraphAddNode(&ifn, graph, &kn, 1, &ip)) != cudaSuccess) break;
+    cudaGraph_t body = ip.conditional.phGraph_out[0];
+    cudaGraphNode_t last, loop;
+    if (add) {
+      rc = add_level_loop<A, W>(g, body, nullptr, 0, cfg, &loop);
+    } else {
+      rc = add_del_repair<A, W>(g, body, nullptr, 0, &last);
+      if (!rc) rc = add_level_loop<A, W>(g, body, &last, 1, cfg, &loop);
+    }
+    if (rc) break;
+    cudaGraphNode_t mn;
+    if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &ifn, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
+                                      cudaMemcpyDeviceToHost)) != cudaSuccess)
+      break;
+    e = cudaGraphInstantiate(&slot.exec, graph, 0);
+  } while (0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    slot.exec = nullptr;
+    return cuda_fail(e, "building the fused apply graph");
+  }
+  if (rc) {
+    slot.exec = nullptr;
+    return rc;
+  }
+  slot.key = key;
+  *out = slot.exec;
+  return RG_OK;
+}
+
+template <int A, bool W>
+int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
+                  uint64_t *old_num) {
+  int rc = storage_reserve(g, 2 * SMALL_EDGES);  // op arrays and staging sized once for the small path
+  if (rc) return rc;
+  char *st = reinterpret_cast<char *>(g.stage_host);
+  ApplyHdr *h = reinterpret_cast<ApplyHdr *>(st);
+  std::memcpy(st + APPLY_DATA_OFF, pairs ? (const void *)pairs : (const void *)edges,
+              n * (pairs ? 16 : sizeof(rg_edge)));
+  h->n = n;
+  h->pairs = pairs ? 1 : 0;
+  h->want_old = old_num ? 1 : 0;
+  h->inv_tag = 0;
+  g.adj_version++;
+  if ((rc = guard_counters(g))) return rc;
+  if (!add) {
+    if (++g.inv_epoch >= 0x7FFFFFFFu) {
+      RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+      g.inv_epoch = 1;
+    }
+    h->inv_tag = 2ull * g.inv_epoch;  // tag: invalidated; tag+1: rescued
+  }
+  reset_stats(g);
+  cudaGraphExec_t exec;
+  if ((rc = apply_exec<A, W>(g, add, directed, &exec))) return rc;
+  count_launch(g);
+  RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  const int what = add ? 1 : 2;
+  bool replayed = false;
+  if (add && g.h_ctl[C_ERR] == RG_ENOSPACE && g.h_ctl[C_AUX] == 1) {
+    // growth ran out of pool: compact, then replay from the growth step
+    const uint64_t nops = directed ? n : 2 * n;
+    rc = storage_recover(g);
+    if (!rc) rc = storage_replay(g, n, nops, directed, true);
+    if (!rc) rc = dispatch(g, A, what, n, directed, true, 0);
+    if (!rc && old_num) rc = storage_copy_old(g, n);
+    if (!rc) rc = sync_ctl(g);
+    if (rc) return rc;
+    replayed = true;
+  }
+  if ((rc = storage_error(g))) return rc;
+  if ((rc = after_sync<A, W>(g, what))) return rc;
+  if (old_num) std::memcpy(old_num, replayed ? (const void *)storage_old_host(g) : (const void *)(st + apply_old_off()),
+                           n * 8);
+  return RG_OK;
+}
+
+int apply_small(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
+                uint64_t *old_num) {
+  const bool W = g.weighted != 0;
+  switch (g.algo) {
+    case RG_BFS: return W ? apply_small_t<RG_BFS, true>(g, edges, pairs, n, directed, add, old_num)
+                          : apply_small_t<RG_BFS, false>(g, edges, pairs, n, directed, add, old_num);
+    case RG_SSSP: return W ? apply_small_t<RG_SSSP, true>(g, edges, pairs, n, directed, add, old_num)
+                           : apply_small_t<RG_SSSP, false>(g, edges, pairs, n, directed, add, old_num);
+    case RG_SSWP: return W ? apply_small_t<RG_SSWP, true>(g, edges, pairs, n, directed, add, old_num)
+                           : apply_small_t<RG_SSWP, false>(g, edges, pairs, n, directed, add, old_num);
+    case RG_WCC: return W ? apply_small_t<RG_WCC, true>(g, edges, pairs, n, directed, add, old_num)
+                          : apply_small_t<RG_WCC, false>(g, edges, pairs, n, directed, add, old_num);
+  }
+  set_error("labels were not built (call rg_build_tree first)");
+  return RG_ESTATE;
 }
 
 int tree_classify(Graph &g, uint64_t n, int directed, const uint8_t *is_del_dev, uint8_t *unsafe_dev) {
