@@ -13,6 +13,11 @@ value  = reached edges / device time per build (GTEPS), CUDA events on the
 e2e    = the same through the public API with the result read back: every
          step calls rg_build_tree and copies the value array into pinned host
          memory; wall clock.
+served = (N=1) the served incremental path: closed-loop clients stream sliding-
+         window inserts and deletes of an RMAT-24 SSSP instance through the
+         rg_server API (host buffers in, completions out); best updates/s at
+         p99 <= 1 ms for the batched server and for the plain one-update-per-
+         launch path, and their ratio.
 --impl reference runs the reference's own CPU build_tree (oracle/_ref, the
 reference's core/graph.hpp compiled with an OpenMP stand-in for TBB) on the
 host cores.  Multi-GPU: independent replicas, one per rank (the path does not
@@ -46,7 +51,7 @@ THROTTLE_BITS = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=22)
@@ -54,6 +59,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-timeout", type=float, default=240.0)
+    ap.add_argument("--served-scale", type=int, default=24, help="RMAT scale of the served instance (0 = skip)")
+    ap.add_argument("--served-seconds", type=float, default=1.0, help="load duration per client count")
+    ap.add_argument("--think-us", type=float, default=50.0, help="mean exponential think time per client")
     return ap.parse_args()
 
 
@@ -114,6 +122,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0:  # nvidia-smi start-up
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -193,6 +204,61 @@ def run_reference(args):
                                        f"{args.warmup} warm-up (load {info['load_s']:.1f}s untimed)"},
             "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def served_leg(args):
+    """Served incremental SSSP: closed-loop clients with Poisson think times
+    send sliding-window inserts and deletes to a resident RMAT instance; the
+    client count doubles until p99 passes 1 ms.  Both the batched server and
+    the plain one-update-per-launch path run the same sweep; each reports its
+    best updates/s with p99 <= 1 ms.  After the sweeps, the incrementally
+    maintained distances must equal a from-scratch build of the final graph."""
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    scale = args.served_scale
+    pairs = gen.rmat(scale, seed=args.seed)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = rg.Graph(V, len(pairs), weighted=True)
+    g.add_pairs(pairs[:imported], True, want_old=False)
+    g.build_tree("sssp", root)
+    offset = 0
+    out = {"workload": f"served incremental SSSP, RMAT-{scale} (V=2^{scale}, E=16*V), first 90% loaded, "
+                       f"sliding-window insert+delete updates, closed-loop clients with exponential think time "
+                       f"{args.think_us:g} us, {args.served_seconds:g} s per client count, clients doubled until "
+                       f"p99 > 1 ms", "device_bytes": g.device_bytes()}
+    for mode, per_update in (("per_update", True), ("served", False)):
+        sweep, best = [], None
+        with rg.Server(per_update=per_update, max_epoch=1 << 16, target_epoch_ms=0.4) as srv:
+            k = srv.attach(g)
+            c = 1
+            while c <= 8192:
+                r, = srv.run_load([dict(instance=k, clients=c, pairs=pairs, imported=imported,
+                                        duration_s=args.served_seconds, think_us=args.think_us, weighted=True,
+                                        offset=offset, seed=c)])
+                offset += r["adds"] + r["dels"]
+                pt = {"clients": c, "updates_per_s": r["updates_per_s"], "p50_us": r["p50_us"],
+                      "p99_us": r["p99_us"], "p999_us": r["p999_us"], "mean_epoch": r["mean_epoch"],
+                      "failed": r["failed"]}
+                sweep.append(pt)
+                if r["failed"]:
+                    break
+                if r["p99_us"] <= 1000.0 and (best is None or r["updates_per_s"] > best["updates_per_s"]):
+                    best = pt
+                if r["p99_us"] > 1000.0 and c >= 4:
+                    break
+                c *= 2
+            srv.detach(k)
+        out[mode] = {"best_at_p99_le_1ms": best, "sweep": sweep}
+    inc = g.values()
+    g.build_tree("sssp", root)
+    out["incremental_equals_rebuild"] = bool(np.array_equal(inc, g.values()))
+    out["updates_applied"] = offset
+    b0, b1 = out["per_update"]["best_at_p99_le_1ms"], out["served"]["best_at_p99_le_1ms"]
+    out["served_over_per_update"] = (b1["updates_per_s"] / b0["updates_per_s"]) if b0 and b1 else None
+    g.close()
+    return out
 
 
 def main():
@@ -280,7 +346,8 @@ def main():
     peak, peak_kind = load_peaks()
     achieved = alg / (push_ms_per_build / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": peak_kind, "traffic": None, "kernel": "k_push+k_push_hub (all levels of one build)",
+            "peak_source": peak_kind, "traffic": None,
+            "kernel": "level kernels of one build (k_level_begin + the level mode's push/pull kernels, all levels)",
             "algorithmic_bytes": alg, "launches_per_build": plaunch / nb, "kernel_ms_per_build": push_ms_per_build}
 
     cpu = None
@@ -296,6 +363,9 @@ def main():
                    "sample": f"RMAT-{args.scale} {algo} build_tree x2 after 1 warm-up "
                              f"(load {info['load_s']:.1f}s untimed)", "values_match_gpu": ok}
 
+    g.close()
+    served = served_leg(args) if (rank == 0 and world == 1 and args.served_scale) else None
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -303,9 +373,8 @@ def main():
                 "config": workload(args), "clocks": clk.summary(),
                 "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": V * 8},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "reached": {"V_r": V_r, "E_r": E_r}}
+                "reached": {"V_r": V_r, "E_r": E_r}, "served": served}
         print(json.dumps(line))
-    g.close()
     if dist:
         dist.destroy_process_group()
 
