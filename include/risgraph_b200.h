@@ -261,7 +261,10 @@ int rg_server_destroy(rg_server *s);
  * duration_s seconds or max_updates updates (0 = no cap), or when the window
  * reaches the end of `pairs`, and returns once all issued updates completed.
  * Every delete removes a loaded copy, so the final graph, and hence the final
- * values, depend only on the number of updates issued, not on their order. */
+ * values, depend only on the number of updates issued, not on their order.
+ * open_loop = 1 makes each client an open Poisson source instead: it issues at
+ * exponential intervals of mean think_us whether or not its earlier updates
+ * have completed (the offered load no longer adapts to the server). */
 typedef struct {
   uint32_t instance;
   uint32_t clients;
@@ -272,7 +275,10 @@ typedef struct {
   const uint64_t *pairs;
   uint64_t n_pairs, imported;
   int weighted;
+  int open_loop;
   uint64_t seed;
+  uint64_t *latencies_ns;  /* optional: every completed update's latency, in completion order */
+  uint64_t latencies_cap;
 } rg_load_config;
 
 typedef struct {

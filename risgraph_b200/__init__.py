@@ -47,7 +47,8 @@ class LoadConfig(ctypes.Structure):  # rg_load_config
                 ("duration_s", ctypes.c_double), ("max_updates", ctypes.c_uint64), ("offset", ctypes.c_uint64),
                 ("pairs", ctypes.c_void_p),
                 ("n_pairs", ctypes.c_uint64), ("imported", ctypes.c_uint64), ("weighted", ctypes.c_int),
-                ("seed", ctypes.c_uint64)]
+                ("open_loop", ctypes.c_int), ("seed", ctypes.c_uint64), ("latencies_ns", ctypes.c_void_p),
+                ("latencies_cap", ctypes.c_uint64)]
 
 
 class LoadResult(ctypes.Structure):  # rg_load_result
@@ -474,7 +475,7 @@ class Server:
 
     def run_load(self, loads) -> list[dict]:
         """loads: dicts with instance, clients, pairs (uint64 (n,2)), imported,
-        and optionally think_us, duration_s, max_updates, offset, weighted, seed."""
+        and optionally think_us, duration_s, max_updates, offset, weighted, open_loop, seed."""
         keep = []
         cfgs = (LoadConfig * len(loads))()
         for i, d in enumerate(loads):
@@ -482,8 +483,8 @@ class Server:
             keep.append(pairs)
             cfgs[i] = LoadConfig(int(d["instance"]), int(d["clients"]), float(d.get("think_us", 0.0)),
                                  float(d.get("duration_s", 1.0)), int(d.get("max_updates", 0)),
-                                 int(d.get("offset", 0)), pairs.ctypes.data, len(pairs), int(d["imported"]), int(d.get("weighted", 0)),
-                                 int(d.get("seed", 1)))
+                                 int(d.get("offset", 0)), pairs.ctypes.data, len(pairs), int(d["imported"]),
+                                 int(d.get("weighted", 0)), int(d.get("open_loop", 0)), int(d.get("seed", 1)), None, 0)
         res = (LoadResult * len(loads))()
         _check(lib().rg_server_run_load(self._h, cfgs, len(loads), res), "rg_server_run_load")
         return [_struct_dict(r) for r in res]

@@ -16,6 +16,10 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "librisgraph_b200.so")
+BIN = os.path.join(PKG, "bin")
+DRIVER = os.path.join(BIN, "rg_driver")
+# the reference's command-line drivers, all served by one binary (argv[0] picks)
+DRIVER_NAMES = [a + m for a in ("bfs", "sssp", "sswp", "wcc") for m in ("", "_inc", "_inc_batch", "_inc_rt")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++"
@@ -26,7 +30,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompi
 
 CU_SOURCES = ["rg_api.cu", "rg_storage.cu", "rg_tree.cu", "rg_static.cu", "rg_serve.cu"]
 C_SOURCES = ["rg_gen.c"]
-HEADERS = ["rg_internal.cuh"]
+HEADERS = ["rg_internal.cuh", "rg_storage_dev.cuh"]
 
 
 def _newer(target, deps):
@@ -67,7 +71,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if force or _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", LIB] + objs +
              ["-Xcompiler", "-fopenmp", "-lgomp", "-cudart", "static"], verbose)
+    build_drivers(verbose, force)
     return LIB
+
+
+def build_drivers(verbose: bool = False, force: bool = False) -> str:
+    """risgraph_b200/bin/rg_driver and its links bfs, sssp_inc, wcc_inc_rt, ..."""
+    os.makedirs(BIN, exist_ok=True)
+    src = os.path.join(PKG, "cli", "rg_driver.cpp")
+    if force or _newer(DRIVER, [src, LIB, os.path.join(INCLUDE, "risgraph_b200.h")]):
+        _run([HOST_CXX, "-std=c++17", "-O2", "-fopenmp", "-I" + INCLUDE, src, "-L" + PKG, "-lrisgraph_b200",
+              "-Wl,-rpath,$ORIGIN/..", "-o", DRIVER], verbose)
+    for name in DRIVER_NAMES:
+        link = os.path.join(BIN, name)
+        if not os.path.islink(link):
+            if os.path.exists(link):
+                os.remove(link)
+            os.symlink("rg_driver", link)
+    return DRIVER
 
 
 if __name__ == "__main__":

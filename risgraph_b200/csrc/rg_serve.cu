@@ -197,11 +197,15 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
   const uint32_t C = std::max<uint32_t>(1, c.clients);
   std::mt19937_64 rng(c.seed);
   std::exponential_distribution<double> think(1.0);
-  const double think_ns = c.think_us > 0 ? c.think_us * 1e3 : 0.0;
+  const bool open = c.open_loop != 0;
+  // an open source needs a finite rate
+  const double think_ns = c.think_us > 0 ? c.think_us * 1e3 : (open ? 1e3 : 0.0);
   const uint64_t limit = c.max_updates ? c.max_updates : ~0ull;
   const uint64_t t_start = now_ns();
   const uint64_t t_stop = t_start + (uint64_t)(std::max(0.0, c.duration_s) * 1e9);
   std::vector<uint64_t> next(C, t_start);
+  if (open)
+    for (uint32_t k = 0; k < C; k++) next[k] = t_start + (uint64_t)(think(rng) * think_ns);
   std::vector<char> busy(C, 0);
   std::vector<rg_request> reqs;
   std::vector<rg_completion> got;
@@ -215,7 +219,7 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
     if (issuing) {
       reqs.clear();
       for (uint32_t k = 0; k < C && issuing; k++) {
-        if (busy[k] || next[k] > now) continue;
+        if ((!open && busy[k]) || next[k] > now) continue;
         const uint64_t sn = c.offset + issued;
         const bool is_add = (sn & 1) == 0;
         const uint64_t idx = is_add ? c.imported + sn / 2 : sn / 2;
@@ -225,7 +229,8 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
         }
         const uint64_t u = c.pairs[2 * idx], v = c.pairs[2 * idx + 1];
         reqs.push_back(rg_request{in->id, is_add ? 0u : 1u, u, v, c.weighted ? rg_gen_weight(u, v) : 0, k});
-        busy[k] = 1;
+        if (open) next[k] += (uint64_t)(think(rng) * think_ns);  // Poisson arrivals, independent of completions
+        else busy[k] = 1;
         issued++;
       }
       if (!reqs.empty()) {
@@ -245,7 +250,7 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
     uint64_t wake = ~0ull;
     if (issuing)
       for (uint32_t k = 0; k < C; k++)
-        if (!busy[k]) wake = std::min(wake, next[k]);
+        if (open || !busy[k]) wake = std::min(wake, next[k]);
     {
       std::unique_lock<std::mutex> lk(sink.mu);
       if (sink.items.empty()) {
@@ -265,14 +270,17 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
     }
     for (const rg_completion &d : got) {
       const uint64_t k = d.tag;
-      busy[k] = 0;
       outstanding--;
       r.completed++;
       if (d.status) r.failed++;
+      if (c.latencies_ns && lat.size() < c.latencies_cap) c.latencies_ns[lat.size()] = d.done_ns - d.submit_ns;
       lat.push_back(d.done_ns - d.submit_ns);
       sum_us += (d.done_ns - d.submit_ns) * 1e-3;
       last_done = std::max(last_done, d.done_ns);
-      next[k] = d.done_ns + (uint64_t)(think_ns > 0 ? think(rng) * think_ns : 0.0);
+      if (!open) {
+        busy[k] = 0;
+        next[k] = d.done_ns + (uint64_t)(think_ns > 0 ? think(rng) * think_ns : 0.0);
+      }
     }
   }
   std::sort(lat.begin(), lat.end());

@@ -136,3 +136,15 @@ def test_hbm_admission():
 
 def gen_w(u, v):
     return int(rg.lib().rg_gen_weight(u, v))
+
+
+def test_open_loop_poisson_load():
+    inst = make_instance("wcc", 12, 12)
+    with rg.Server(max_epoch=1024) as srv:
+        k = srv.attach(inst["g"], directed=False)
+        load = load_of(inst, k, 16, 1500, 3)
+        load.update(open_loop=1, think_us=200.0)
+        r, = srv.run_load([load])
+        srv.detach(k)
+    assert r["completed"] == 1500 and r["failed"] == 0
+    np.testing.assert_array_equal(inst["g"].values(), expected_values(inst, r["adds"], r["dels"]))
