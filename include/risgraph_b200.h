@@ -156,10 +156,13 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
 /* Strategy knobs of the level engine (the reference hard-codes its own:
  * push/pull switch at core/graph.hpp:334, vertex- vs edge-centric cost model
  * at :595-612, recompute threshold at :1252).  Values are per graph.
- *   RG_OPT_DENSE_PULL     1: dense levels pull over in-edges; 0: edge-centric push
+ *   RG_OPT_DENSE_PULL     dense build levels: 1 pull over in-edges, 0 edge-centric
+ *                         push, 2 (default) pull for WCC and push otherwise
  *   RG_OPT_DENSE_DIV      a level is dense when frontier * div >= |V|
  *   RG_OPT_LBS_MIN        frontiers at least this large use the edge-balanced push
- *   RG_OPT_BFS_BOTTOM_UP  1: full BFS builds pull bottom-up on dense levels
+ *   RG_OPT_BFS_BOTTOM_UP  1: full BFS builds pull bottom-up on large levels
+ *   RG_OPT_BFS_BU_DIV     a BFS build level goes bottom-up when frontier * div >= |V|
+ *                         (default 64; Beamer's direction switch by frontier size)
  *   RG_OPT_RECOMPUTE_MIN  deletion repair falls back to a full build when the
  *                         invalidated set exceeds max(this, |V|/20) */
 typedef enum {
@@ -167,7 +170,8 @@ typedef enum {
   RG_OPT_DENSE_DIV = 1,
   RG_OPT_LBS_MIN = 2,
   RG_OPT_BFS_BOTTOM_UP = 3,
-  RG_OPT_RECOMPUTE_MIN = 4
+  RG_OPT_RECOMPUTE_MIN = 4,
+  RG_OPT_BFS_BU_DIV = 5
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

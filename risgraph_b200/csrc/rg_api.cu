@@ -446,11 +446,15 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
   if (!gh) return RG_EINVAL;
   Graph &g = gh->g;
   switch (option) {
-    case RG_OPT_DENSE_PULL: g.dense_pull = value ? 1 : 0; return RG_OK;
+    case RG_OPT_DENSE_PULL:
+      if (value > 2) return RG_EINVAL;
+      g.dense_pull = (int)value;
+      return RG_OK;
     case RG_OPT_DENSE_DIV: g.dense_div = value ? value : 1; return RG_OK;
     case RG_OPT_LBS_MIN: g.lbs_min = value; return RG_OK;
     case RG_OPT_BFS_BOTTOM_UP: g.bfs_bottom_up = value ? 1 : 0; return RG_OK;
     case RG_OPT_RECOMPUTE_MIN: g.recompute_min = value; return RG_OK;
+    case RG_OPT_BFS_BU_DIV: g.bu_div = value ? value : 1; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -465,6 +469,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_LBS_MIN: *value = g.lbs_min; return RG_OK;
     case RG_OPT_BFS_BOTTOM_UP: *value = (uint64_t)g.bfs_bottom_up; return RG_OK;
     case RG_OPT_RECOMPUTE_MIN: *value = g.recompute_min; return RG_OK;
+    case RG_OPT_BFS_BU_DIV: *value = g.bu_div; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

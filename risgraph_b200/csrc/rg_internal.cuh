@@ -262,9 +262,10 @@ struct Graph {
   uint64_t *pull_P = nullptr, *pull_base = nullptr;
   uint32_t *pull_tile = nullptr;
   uint64_t adj_version = 1, pull_version = 0;
-  int dense_pull = 1;  // dense levels: 1 = pull over in-edges, 0 = edge-centric push
+  int dense_pull = 2;  // dense build levels: 1 = pull over in-edges, 0 = edge-centric push, 2 = pull for WCC only
   uint64_t dense_div = 20, lbs_min = 2048, recompute_min = 2000000;
   int bfs_bottom_up = 1;
+  uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
   LoopGraph loops[16];
   LoopGraph dels[8];

@@ -206,25 +206,41 @@ __global__ void __launch_bounds__(TPB) k_push_hub(DevGraph g, const uint64_t *hu
 }
 
 // Relaxation of N independent candidate edges held by one thread (u[k] -> v[k]
-// with weight w[k], source value su[k], target record cur[k] already loaded).
-// All CASes are issued before any result is used, then all stamp exchanges,
-// then one warp-wide append for every new frontier entry of the warp: the
-// success path costs three round trips per N edges instead of three per edge.
+// with weight w[k], source value su[k]), in two steps.
+// relax_filter reads the 32-bit value mirror of every target and keeps the
+// candidates whose update_func value improves it; it returns whether any lane
+// of the warp kept one, so a warp whose candidates all fail (the common case
+// in late levels) skips the commit entirely.
 template <int A, int N>
-__device__ __forceinline__ void relax_batch(const DevGraph &g, const bool (&on)[N], const uint32_t (&u)[N],
-                                            const uint32_t (&v)[N], const uint32_t (&w)[N],
-                                            const uint64_t (&su)[N], uint32_t st, uint32_t *fout,
-                                            unsigned long long *fout_n, unsigned long long &local, uint32_t mst) {
-  bool pend[N], upd[N];
-  ulonglong2 want[N], old[N], cur[N];
+__device__ __forceinline__ bool relax_filter(const DevGraph &g, bool (&on)[N], const uint32_t (&v)[N],
+                                             const uint32_t (&w)[N], const uint64_t (&su)[N]) {
   uint64_t dv[N];
 #pragma unroll
   for (int k = 0; k < N; k++) dv[k] = on[k] ? ld_v32(g.val32, v[k]) : 0;
+  bool any = false;
 #pragma unroll
   for (int k = 0; k < N; k++) {
-    const uint64_t nv = Hook<A>::combine(su[k], w[k]);
-    pend[k] = on[k] && Hook<A>::better(nv, dv[k]);
-    want[k] = make_ulonglong2(nv, pack_parent(u[k], w[k]));
+    on[k] = on[k] && Hook<A>::better(Hook<A>::combine(su[k], w[k]), dv[k]);
+    any |= on[k];
+  }
+  return __any_sync(FULL, any);
+}
+
+// relax_commit (all lanes of the warp): issues every CAS of the kept
+// candidates before any result is used, then the stamp exchanges, then one
+// warp-wide append for every new frontier entry of the warp, so the success
+// path costs three round trips per N edges instead of three per edge.
+template <int A, int N>
+__device__ __forceinline__ void relax_commit(const DevGraph &g, const bool (&on)[N], const uint32_t (&u)[N],
+                                             const uint32_t (&v)[N], const uint32_t (&w)[N],
+                                             const uint64_t (&su)[N], uint32_t st, uint32_t *fout,
+                                             unsigned long long *fout_n, unsigned long long &local, uint32_t mst) {
+  bool pend[N], upd[N];
+  ulonglong2 want[N], old[N], cur[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    pend[k] = on[k];
+    want[k] = make_ulonglong2(Hook<A>::combine(su[k], w[k]), pack_parent(u[k], w[k]));
     upd[k] = false;
   }
 #pragma unroll
@@ -284,6 +300,17 @@ __device__ __forceinline__ void relax_batch(const DevGraph &g, const bool (&on)[
 #pragma unroll
     for (int k = 0; k < N; k++) mark_modified(g, upd[k], v[k], mst);
   }
+}
+
+template <int A, int N>
+__device__ __forceinline__ void relax_batch(const DevGraph &g, const bool (&on)[N], const uint32_t (&u)[N],
+                                            const uint32_t (&v)[N], const uint32_t (&w)[N],
+                                            const uint64_t (&su)[N], uint32_t st, uint32_t *fout,
+                                            unsigned long long *fout_n, unsigned long long &local, uint32_t mst) {
+  bool keep[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) keep[k] = on[k];
+  if (relax_filter<A, N>(g, keep, v, w, su)) relax_commit<A, N>(g, keep, u, v, w, su, st, fout, fout_n, local, mst);
 }
 
 // ---- edge-balanced push for large frontiers -------------------------------
@@ -506,9 +533,13 @@ __global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint
       const uint64_t i = base + (uint64_t)k * DN_TPB + threadIdx.x;
       o[k] = i < slots ? __ldg(&g.out.owner[i]) : NONE;
     }
-    bool a[DN_ITEMS];
+    bool a[DN_ITEMS], any = false;
 #pragma unroll
-    for (int k = 0; k < DN_ITEMS; k++) a[k] = o[k] != NONE && __ldg(&act[o[k]]) == act_id;
+    for (int k = 0; k < DN_ITEMS; k++) {
+      a[k] = o[k] != NONE && __ldg(&act[o[k]]) == act_id;
+      any |= a[k];
+    }
+    if (!__any_sync(FULL, any)) continue;  // no active owner in the warp's slots
     uint32_t vv[DN_ITEMS], ww[DN_ITEMS];
     uint64_t su[DN_ITEMS];
 #pragma unroll
@@ -762,6 +793,7 @@ __host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
 struct LevelCfg {
   uint64_t dense_div;
   uint64_t lbs_min;
+  uint64_t bu_div;  // BFS builds go bottom-up once frontier * bu_div >= |V|
   int allow_pull;
   int bottom_up;
 };
@@ -781,7 +813,7 @@ __global__ void k_level_begin(DevGraph g, const unsigned long long *fin_n, unsig
   const bool dense = n * cfg.dense_div >= g.V;
   unsigned long long mode = M_SPARSE;
   if (n == 0) mode = M_EMPTY;
-  else if (dense && cfg.bottom_up) mode = M_BOTTOM_UP;
+  else if (cfg.bottom_up && n * cfg.bu_div >= g.V) mode = M_BOTTOM_UP;
   else if (dense && cfg.allow_pull) mode = M_PULL;
   else if (dense) mode = M_DENSE_PUSH;
   else if (n >= cfg.lbs_min) mode = M_LBS;
@@ -1255,8 +1287,12 @@ int guard_counters(Graph &g) {
 }
 
 // In-edge partition for dense pull levels, rebuilt only after the adjacency changed.
+// Dense build levels pull for WCC by default (measured faster there; push wins
+// for BFS / SSSP / SSWP); RG_OPT_DENSE_PULL 0 / 1 force push / pull.
+bool pull_on(const Graph &g, int A) { return g.dense_pull == 1 || (g.dense_pull == 2 && A == RG_WCC); }
+
 int prepare_pull(Graph &g) {
-  if (!g.dense_pull || g.pull_version == g.adj_version) return RG_OK;
+  if (g.pull_version == g.adj_version) return RG_OK;
   count_launch(g, 5);
   k_in_degrees<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.scratch64);
   size_t tb = g.cub_tmp_bytes;
@@ -1311,8 +1347,9 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   LevelCfg cfg;
   cfg.dense_div = g.dense_div;
   cfg.lbs_min = g.lbs_min;
-  cfg.allow_pull = (build_variant && g.dense_pull) ? 1 : 0;
+  cfg.allow_pull = (build_variant && pull_on(g, A)) ? 1 : 0;
   cfg.bottom_up = (A == RG_BFS && build_variant && g.bfs_bottom_up) ? 1 : 0;
+  cfg.bu_div = g.bu_div;
   return cfg;
 }
 
@@ -1461,7 +1498,7 @@ template <int A, bool W>
 int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
   const LevelCfg cfg = level_cfg(g, A, build_variant);
   LoopGraph &slot = g.loops[(A * 2 + (W ? 1 : 0)) * 2 + (build_variant ? 1 : 0)];
-  const uint64_t key = (g.layout_version << 40) ^ (cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^
+  const uint64_t key = (g.layout_version << 40) ^ (cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^ (cfg.bu_div << 28) ^
                        ((uint64_t)cfg.allow_pull << 1) ^ (uint64_t)cfg.bottom_up;
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
@@ -1495,7 +1532,7 @@ int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
 // so each level can be timed.
 template <int A, bool W>
 int push_levels(Graph &g, bool build_variant) {
-  if (build_variant) {
+  if (build_variant && pull_on(g, A)) {
     int rc = prepare_pull(g);
     if (rc) return rc;
   }
