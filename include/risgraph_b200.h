@@ -156,8 +156,12 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
 /* Strategy knobs of the level engine (the reference hard-codes its own:
  * push/pull switch at core/graph.hpp:334, vertex- vs edge-centric cost model
  * at :595-612, recompute threshold at :1252).  Values are per graph.
- *   RG_OPT_DENSE_PULL     dense build levels: 1 pull over in-edges, 0 edge-centric
- *                         push, 2 (default) pull for WCC and push otherwise
+ *   RG_OPT_DENSE_PULL     build levels may pull over in-edges: 1 always, 0 never,
+ *                         2 (default) for SSSP / SSWP / WCC (BFS goes bottom-up)
+ *   RG_OPT_PULL_DIV       a build level pulls when frontier * div >= |V| (default 64)
+ *   RG_OPT_TINY_EDGES     frontiers of at most 1024 vertices and this many out-slots
+ *                         run level after level in one CTA (default 32768, max 2^20,
+ *                         0 = off)
  *   RG_OPT_DENSE_DIV      a level is dense when frontier * div >= |V|
  *   RG_OPT_LBS_MIN        frontiers at least this large use the edge-balanced push
  *   RG_OPT_BFS_BOTTOM_UP  1: full BFS builds pull bottom-up on large levels
@@ -171,7 +175,9 @@ typedef enum {
   RG_OPT_LBS_MIN = 2,
   RG_OPT_BFS_BOTTOM_UP = 3,
   RG_OPT_RECOMPUTE_MIN = 4,
-  RG_OPT_BFS_BU_DIV = 5
+  RG_OPT_BFS_BU_DIV = 5,
+  RG_OPT_PULL_DIV = 6,
+  RG_OPT_TINY_EDGES = 7
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

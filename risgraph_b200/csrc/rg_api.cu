@@ -198,7 +198,8 @@ int rg_destroy(rg_graph *gh) {
   cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
   cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp); cudaFree(g.act);
-  cudaFree(g.pull_P); cudaFree(g.pull_base); cudaFree(g.pull_tile); cudaFree(g.lb_sums);
+  cudaFree(g.sell_ent); cudaFree(g.sell_off); cudaFree(g.sell_row); cudaFree(g.sell_hub); cudaFree(g.sell_piece);
+  cudaFree(g.sell_cnt); cudaFree(g.sell_hub_off); cudaFree(g.sell_piece_best); cudaFree(g.lb_sums);
   if (g.h_ctl) cudaFreeHost(g.h_ctl);
   if (g.pev[0]) cudaEventDestroy(g.pev[0]);
   if (g.pev[1]) cudaEventDestroy(g.pev[1]);
@@ -455,6 +456,8 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
     case RG_OPT_BFS_BOTTOM_UP: g.bfs_bottom_up = value ? 1 : 0; return RG_OK;
     case RG_OPT_RECOMPUTE_MIN: g.recompute_min = value; return RG_OK;
     case RG_OPT_BFS_BU_DIV: g.bu_div = value ? value : 1; return RG_OK;
+    case RG_OPT_PULL_DIV: g.pull_div = value ? value : 1; return RG_OK;
+    case RG_OPT_TINY_EDGES: g.tiny_edges = value; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -470,6 +473,8 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_BFS_BOTTOM_UP: *value = (uint64_t)g.bfs_bottom_up; return RG_OK;
     case RG_OPT_RECOMPUTE_MIN: *value = g.recompute_min; return RG_OK;
     case RG_OPT_BFS_BU_DIV: *value = g.bu_div; return RG_OK;
+    case RG_OPT_PULL_DIV: *value = g.pull_div; return RG_OK;
+    case RG_OPT_TINY_EDGES: *value = g.tiny_edges; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

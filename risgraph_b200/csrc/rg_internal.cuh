@@ -70,11 +70,12 @@ enum Ctl : int {
 enum LevelMode : unsigned long long {
   M_EMPTY = 0,      // frontier empty: every level kernel returns at once
   M_SPARSE = 1,     // k_push + k_push_hub over the frontier list
-  M_PULL = 2,       // k_pull_dense over all in-edges
+  M_PULL = 2,       // k_pull_hubs + k_pull_sell over all in-edges
   M_DENSE_PUSH = 3, // k_push_dense over all out-slots of active vertices
   M_BOTTOM_UP = 4,  // k_bfs_bottom_up (full BFS builds)
   M_LBS = 5,        // edge-balanced push (degree scan + tile partition + k_push_lbs)
-  M_COUNT = 6
+  M_TINY = 6,       // k_push_tiny: one CTA runs successive small levels
+  M_COUNT = 7
 };
 constexpr int TRACE_CAP = 4096;
 
@@ -258,9 +259,23 @@ struct Graph {
   uint64_t *lb_sums = nullptr;    // per-block sums of the device-side frontier scan
   uint32_t *act = nullptr;        // V: level id of the dense level a vertex is active in
   uint32_t act_epoch = 0;
-  // static in-edge partition for dense pull levels, valid while adj_version == pull_version
-  uint64_t *pull_P = nullptr, *pull_base = nullptr;
-  uint32_t *pull_tile = nullptr;
+  // sliced-ELL copy of the in-edges for dense pull levels, valid while adj_version == pull_version
+  void *sell_ent = nullptr;       // entries, slice-major, column-major inside a slice
+  uint64_t sell_cap = 0;          // entries allocated
+  uint64_t *sell_off = nullptr;   // slice offsets (entries), slices + 1
+  uint32_t *sell_row = nullptr;   // row ids by length, descending: vertex id, or |V| + hub piece index
+  uint64_t sell_row_cap = 0;
+  uint32_t *sell_hub = nullptr;   // hub vertices (in-list longer than a row)
+  uint64_t sell_hub_cap = 0;
+  uint64_t *sell_hub_off = nullptr;  // first piece of each hub (prefix of piece counts)
+  uint32_t *sell_piece = nullptr;  // pieces: vertex[P+1], start[P+1], length[P+1]
+  uint64_t sell_piece_cap = 0;
+  ulonglong2 *sell_piece_best = nullptr;  // best {value, parent | w << 32} of each piece in a pull level
+  uint64_t sell_best_cap = 0;
+  unsigned long long *sell_cnt = nullptr;
+  uint64_t sell_hubs = 0, sell_rows = 0, sell_slices = 0, sell_epoch = 0;
+  uint64_t pull_div = 64;
+  uint64_t tiny_edges = 32768;  // frontiers with at most this many out-slots run in k_push_tiny (0: off)
   uint64_t adj_version = 1, pull_version = 0;
   int dense_pull = 2;  // dense build levels: 1 = pull over in-edges, 0 = edge-centric push, 2 = pull for WCC only
   uint64_t dense_div = 20, lbs_min = 2048, recompute_min = 2000000;

@@ -24,6 +24,7 @@
 
 #include <cub/block/block_reduce.cuh>
 #include <cub/block/block_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "rg_internal.cuh"
@@ -36,7 +37,6 @@ namespace {
 constexpr int TPB = 256;
 constexpr uint32_t HUB = 64;     // longer lists of a small frontier are split into
 constexpr uint32_t CHUNK = 64;   // CHUNK-slot tasks so no warp walks a long list alone
-constexpr uint64_t LBS_MIN_FRONTIER = 2048;  // smaller frontiers use k_push
 
 template <bool W>
 struct PoolT;
@@ -564,151 +564,266 @@ __global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint
 
 // ---- dense pull over in-edges ----------------------------------------------
 // The reference's dense mode (stream_edges dense lambda, core/graph.hpp:936-976):
-// every vertex takes the best update_func value over its in-edges.  The whole
-// in-edge range is partitioned once per tree call into PL_TILE-edge tiles
-// (prefix of in-degrees over all vertices, which does not change during the
-// call); a thread reads PL_ITEMS in-edges and their source values, a segmented
-// warp reduction keeps the best candidate per destination, and only the first
-// lane of each destination run issues a CAS.  Per in-edge: one coalesced entry
-// read and one source-value read; no atomics.
-constexpr int PL_TPB = 256;
-constexpr int PL_ITEMS = 4;
-constexpr uint32_t PL_TILE = PL_TPB * PL_ITEMS;
-constexpr uint32_t PL_CAP = PL_TILE + 1;
+// every vertex takes the best update_func value over its in-edges.  For full
+// builds the live in-edges are copied once per adjacency version into a sliced
+// ELLPACK layout (SELL-32): rows sorted by length, 32 consecutive rows per
+// slice, a slice stored column-major so that lane l of a warp reads row l and
+// the 32 lanes of a warp read 32 consecutive entries.  A row is a vertex's
+// in-list, or for a hub (in-list longer than PULL_HUB) one of the equal pieces
+// its list is cut into, so every row holds at most PULL_HUB entries and the
+// warps stay balanced.  A pull level is one warp per slice with no search and
+// no atomics on labels: a vertex row is written only by its own lane; a piece
+// leaves its best in a side array and k_pull_hub_fix combines the pieces of
+// each hub.
+constexpr uint32_t PULL_HUB = 1024;
+constexpr int PS_TPB = 256;
+// In-list entries a lane keeps in flight: 16 for 8-byte weighted entries; 8 for
+// 4-byte ones, plus the next 8 prefetched (measured best on RMAT-22).
+template <bool W>
+struct PullDepth {
+  static constexpr int N = W ? 16 : 8;
+  static constexpr bool prefetch = !W;
+};
 
-__global__ void k_in_degrees(DevGraph g, uint64_t *deg) {
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v <= g.V; v += stride)
-    deg[v] = v < g.V ? seg_len(g.in, (uint32_t)v) : 0;
-}
+template <bool W>
+struct SellE;
+template <>
+struct SellE<true> {
+  using E = uint2;
+  static __device__ __forceinline__ E none() { return make_uint2(NONE, 0u); }
+  static __device__ __forceinline__ E make(uint32_t u, uint32_t w) { return make_uint2(u, w); }
+  static __device__ __forceinline__ uint32_t nbr(E e) { return e.x; }
+  static __device__ __forceinline__ uint32_t wt(E e) { return e.y; }
+};
+template <>
+struct SellE<false> {
+  using E = uint32_t;
+  static __device__ __forceinline__ E none() { return NONE; }
+  static __device__ __forceinline__ E make(uint32_t u, uint32_t) { return u; }
+  static __device__ __forceinline__ uint32_t nbr(E e) { return e; }
+  static __device__ __forceinline__ uint32_t wt(E) { return 0u; }
+};
 
-__global__ void k_in_base(DevGraph g, const uint64_t *P, uint64_t *base) {
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.V; v += stride)
-    base[v] = g.in.off[v] - P[v];
-}
+// Pieces of a hub of in-list length len: equal lengths of at most PULL_HUB.
+__device__ __forceinline__ uint32_t hub_pieces(uint32_t len) { return (len + PULL_HUB - 1) / PULL_HUB; }
 
-__global__ void k_partition_tiles(const uint64_t *P, uint64_t n, uint32_t tile_edges, uint32_t *tile_lo) {
-  const uint64_t T = P[n];
-  const uint64_t ntiles = (T + tile_edges - 1) / tile_edges;
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles; t += stride) {
-    uint64_t x = t < ntiles ? t * tile_edges : T;
-    uint64_t lo = 0, hi = n;
-    while (lo < hi) {
-      uint64_t mid = (lo + hi + 1) >> 1;
-      if (__ldg(&P[mid]) <= x) lo = mid;
-      else hi = mid - 1;
+// Hubs (in-list longer than PULL_HUB) with their piece counts.
+__global__ void k_sell_hubs(DevGraph g, uint32_t *hub_v, uint64_t *hub_np, unsigned long long *cnt) {
+  const uint64_t V = g.V;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += stride) {
+    const uint32_t d = seg_len(g.in, (uint32_t)v);
+    if (d > PULL_HUB) {
+      const unsigned long long h = atomicAdd(cnt, 1ull);
+      hub_v[h] = (uint32_t)v;
+      hub_np[h] = hub_pieces(d);
     }
-    tile_lo[t] = (uint32_t)(lo < n ? lo : (n ? n - 1 : 0));
   }
+}
+
+// Row keys of the vertices: in-list length, 0 for hubs (their rows are pieces).
+__global__ void k_sell_keys(DevGraph g, uint32_t *key, uint32_t *id) {
+  const uint64_t V = g.V;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += stride) {
+    const uint32_t d = seg_len(g.in, (uint32_t)v);
+    key[v] = d > PULL_HUB ? 0u : d;
+    id[v] = (uint32_t)v;
+  }
+}
+
+// Piece rows of every hub (id V + piece index), their keys and the piece table.
+__global__ void k_sell_pieces(DevGraph g, const uint32_t *hub_v, const uint64_t *piece_off, uint64_t nh, uint32_t *key,
+                              uint32_t *id, uint32_t *piece_v, uint32_t *piece_start, uint32_t *piece_len) {
+  const uint64_t V = g.V;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t h = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; h < nh; h += stride) {
+    const uint32_t v = hub_v[h];
+    const uint32_t d = seg_len(g.in, v);
+    const uint64_t p0 = piece_off[h];
+    const uint32_t np = hub_pieces(d), base = d / np, extra = d % np;
+    uint32_t start = 0;
+    for (uint32_t k = 0; k < np; k++) {
+      const uint32_t n = base + (k < extra ? 1u : 0u);
+      key[V + p0 + k] = n;
+      id[V + p0 + k] = (uint32_t)(V + p0 + k);
+      piece_v[p0 + k] = v;
+      piece_start[p0 + k] = start;
+      piece_len[p0 + k] = n;
+      start += n;
+    }
+  }
+}
+
+__global__ void k_sell_count(const uint32_t *key, uint64_t n, unsigned long long *rows) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    const unsigned b = __ballot_sync(FULL, i < n && key[i] > 0);
+    if (lane_id() == 0 && b) atomicAdd(rows, (unsigned long long)__popc(b));
+  }
+}
+
+// Slice sizes (entries): 32 x the length of the slice's first (longest) row.
+__global__ void k_sell_sizes(const uint32_t *sorted_key, uint64_t slices, uint64_t *size) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s <= slices; s += stride)
+    size[s] = s < slices ? 32ull * sorted_key[s * 32] : 0;
+}
+
+// Copy the live in-entries of each row into its column; pad with NONE.
+template <bool W>
+__global__ void k_sell_fill(DevGraph g, const uint32_t *row_id, uint64_t rows, uint64_t slices, const uint64_t *off,
+                            const uint32_t *piece_v, const uint32_t *piece_start, const uint32_t *piece_len,
+                            typename SellE<W>::E *ent) {
+  using P_ = PoolT<W>;
+  using S_ = SellE<W>;
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.in.pool);
+  const uint64_t V = g.V;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < slices * 32; r += stride) {
+    const uint64_t s = r >> 5, lane = r & 31;
+    const uint64_t o0 = off[s], width = (off[s + 1] - o0) >> 5;
+    uint64_t j = 0;
+    if (r < rows) {
+      const uint32_t id = row_id[r];
+      uint32_t v, k0, n;
+      if (id < V) {
+        v = id;
+        k0 = 0;
+        n = seg_len(g.in, v);
+      } else {
+        v = piece_v[id - V];
+        k0 = piece_start[id - V];
+        n = piece_len[id - V];
+      }
+      const uint64_t so = g.in.off[v] + k0;
+      for (uint32_t k = 0; k < n && j < width; k++) {
+        const typename P_::E e = pool[so + k];
+        const uint32_t u = P_::nbr(e);
+        if (u & DEAD) continue;
+        ent[o0 + j * 32 + lane] = S_::make(u, P_::wt(e));
+        j++;
+      }
+    }
+    for (; j < width; j++) ent[o0 + j * 32 + lane] = S_::none();
+  }
+}
+
+// Writes v's pulled best when it improves v's value (single writer per vertex).
+template <int A>
+__device__ __forceinline__ bool pull_commit(const DevGraph &g, bool has, uint32_t v, uint64_t best, uint32_t bsrc,
+                                            uint32_t bw) {
+  if (!has || !Hook<A>::better(best, ld_v32(g.val32, v))) return false;
+  g.lab[v] = make_ulonglong2(best, pack_parent(bsrc, bw));
+  g.val32[v] = (uint32_t)best;
+  return true;
 }
 
 template <int A, bool W>
-__global__ void __launch_bounds__(PL_TPB, 3) k_pull_dense(DevGraph g, const uint64_t *P, const uint64_t *base,
-                                                          const uint32_t *tile_lo, uint32_t *fout,
-                                                          unsigned long long *fout_n, uint32_t mst) {
+__global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename SellE<W>::E *ent, const uint64_t *off,
+                                                      const uint32_t *row_id, uint64_t rows, uint64_t slices,
+                                                      ulonglong2 *piece_best, uint32_t *fout,
+                                                      unsigned long long *fout_n, uint32_t mst) {
   if (g.ctl[C_MODE] != M_PULL) return;
-  const uint32_t st = (uint32_t)g.ctl[C_STAMP];
-  using P_ = PoolT<W>;
-  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.in.pool);
-  __shared__ uint32_t s_rel[PL_CAP];
-  __shared__ uint64_t s_base[PL_CAP];
-  const uint64_t V = g.V;
-  const uint64_t T = P[V];
-  const uint64_t ntiles = (T + PL_TILE - 1) / PL_TILE;
+  using S_ = SellE<W>;
   const int lane = lane_id();
+  const uint64_t V = g.V;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long local = 0;
-  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const uint64_t t0 = t * PL_TILE;
-    const uint64_t t1 = min(t0 + PL_TILE, T);
-    const uint32_t lo = tile_lo[t];
-    const uint32_t hi = tile_lo[t + 1];
-    const uint32_t m = hi - lo + 1;
-    const bool staged = m <= PL_CAP;
-    if (staged) {
-      for (uint32_t j = threadIdx.x; j < m; j += PL_TPB) {
-        const uint64_t pj = P[lo + j];
-        s_rel[j] = pj <= t0 ? 0u : (uint32_t)(pj - t0);
-        s_base[j] = base[lo + j];
-      }
-    }
-    __syncthreads();
-    uint32_t dv[PL_ITEMS], src[PL_ITEMS], wt[PL_ITEMS];
-    uint64_t cand[PL_ITEMS], sv[PL_ITEMS];
-    bool ok[PL_ITEMS];
+  for (uint64_t s = warp; s < slices; s += nwarps) {
+    const uint64_t r = s * 32 + lane;
+    const bool active = r < rows;
+    const uint32_t id = active ? row_id[r] : 0u;
+    const uint64_t o0 = off[s], width = (off[s + 1] - o0) >> 5;
+    const typename S_::E *col = ent + o0 + lane;
+    bool has = false;
+    uint64_t best = 0;
+    uint32_t bsrc = 0, bw = 0;
+    constexpr int N = PullDepth<W>::N;
+    typename S_::E ne[N];
+    if constexpr (PullDepth<W>::prefetch) {
 #pragma unroll
-    for (int k = 0; k < PL_ITEMS; k++) {
-      const uint64_t e = t0 + (uint64_t)k * PL_TPB + threadIdx.x;
-      ok[k] = false;
-      dv[k] = NONE;
-      src[k] = 0;
-      wt[k] = 0;
-      if (e < t1) {
-        uint64_t slot;
-        if (staged) {
-          const uint32_t er = (uint32_t)(e - t0);
-          uint32_t a = 0, b = m - 1;
-          while (a < b) {
-            const uint32_t mid = (a + b + 1) >> 1;
-            if (s_rel[mid] <= er) a = mid;
-            else b = mid - 1;
-          }
-          dv[k] = lo + a;
-          slot = s_base[a] + e;
+      for (int k = 0; k < N; k++) ne[k] = k < width ? __ldcs(&col[(uint64_t)k * 32]) : S_::none();
+    }
+    for (uint64_t j = 0; j < width; j += N) {
+      typename S_::E e[N];
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        if constexpr (PullDepth<W>::prefetch) {
+          e[k] = ne[k];
+          ne[k] = j + N + k < width ? __ldcs(&col[(j + N + k) * 32]) : S_::none();
         } else {
-          uint64_t a = lo, b = hi;
-          while (a < b) {
-            const uint64_t mid = (a + b + 1) >> 1;
-            if (P[mid] <= e) a = mid;
-            else b = mid - 1;
-          }
-          dv[k] = (uint32_t)a;
-          slot = base[a] + e;
+          e[k] = j + k < width ? __ldcs(&col[(j + k) * 32]) : S_::none();
         }
-        const typename P_::E ent = __ldg(&pool[slot]);
-        src[k] = P_::nbr(ent);
-        wt[k] = P_::wt(ent);
-        ok[k] = !(src[k] & DEAD);
       }
-    }
+      // Source values through L1: the values of popular sources stay there.
+      // A value cached before its owner improved in this level is only older,
+      // and that owner is in the next frontier anyway.
+      uint64_t sv[N];
 #pragma unroll
-    for (int k = 0; k < PL_ITEMS; k++) sv[k] = ok[k] ? ld_v32(g.val32, src[k]) : 0;
-    bool head[PL_ITEMS];
+      for (int k = 0; k < N; k++) sv[k] = S_::nbr(e[k]) != NONE ? (uint64_t)__ldca(&g.val32[S_::nbr(e[k])]) : 0;
 #pragma unroll
-    for (int k = 0; k < PL_ITEMS; k++) {
-      // segmented best over the warp's run of equal destinations
-      bool has = ok[k];
-      uint64_t c = has ? Hook<A>::combine(sv[k], wt[k]) : 0;
-      uint32_t s = src[k], w = wt[k];
-      uint64_t su = sv[k];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t odv = __shfl_down_sync(FULL, dv[k], o);
-        const bool ohas = __shfl_down_sync(FULL, has, o);
-        const uint64_t oc = __shfl_down_sync(FULL, c, o);
-        const uint32_t os = __shfl_down_sync(FULL, s, o);
-        const uint32_t ow = __shfl_down_sync(FULL, w, o);
-        const uint64_t osu = __shfl_down_sync(FULL, su, o);
-        if (lane + o < 32 && odv == dv[k] && ohas && (!has || Hook<A>::better(oc, c))) {
+      for (int k = 0; k < N; k++) {
+        if (S_::nbr(e[k]) == NONE) continue;
+        const uint64_t c = Hook<A>::combine(sv[k], S_::wt(e[k]));
+        if (!has || Hook<A>::better(c, best)) {
           has = true;
-          c = oc;
-          s = os;
-          w = ow;
-          su = osu;
+          best = c;
+          bsrc = S_::nbr(e[k]);
+          bw = S_::wt(e[k]);
         }
       }
-      const uint32_t pdv = __shfl_up_sync(FULL, dv[k], 1);
-      head[k] = has && dv[k] != NONE && (lane == 0 || pdv != dv[k]);
-      src[k] = s;
-      wt[k] = w;
-      sv[k] = su;
     }
-    relax_batch<A, PL_ITEMS>(g, head, src, dv, wt, sv, st, fout, fout_n, local, mst);
-    __syncthreads();
+    bool upd = false;
+    if (active && id < V) {
+      upd = pull_commit<A>(g, has, id, best, bsrc, bw);
+    } else if (active) {
+      // a hub piece: its best waits for k_pull_hub_fix
+      piece_best[id - V] = make_ulonglong2(best, has ? pack_parent(bsrc, bw) : ~0ull);
+    }
+    local += upd;
+    warp_append(upd, id, fout, fout_n, FULL);
+    if (mst) mark_modified(g, upd, id, mst);
   }
   warp_add_result(local, &g.ctl[C_RESULT]);
-  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&g.ctl[C_EDGES], T);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&g.ctl[C_EDGES], off[slices]);
+}
+
+// One warp per hub: best of its pieces, one write.
+template <int A>
+__global__ void k_pull_hub_fix(DevGraph g, const uint32_t *hub_v, const uint64_t *piece_off, uint64_t nh,
+                               const ulonglong2 *piece_best, uint32_t *fout, unsigned long long *fout_n, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_PULL) return;
+  const int lane = lane_id();
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long local = 0;
+  for (uint64_t h0 = warp * 32; h0 < nh; h0 += nwarps * 32) {
+    // lane l owns hub h0 + l; the warp scans the pieces of its 32 hubs
+    const uint64_t h = h0 + lane;
+    bool has = false;
+    uint64_t best = 0, meta = 0;
+    uint32_t v = 0;
+    if (h < nh) {
+      v = hub_v[h];
+      for (uint64_t p = piece_off[h]; p < piece_off[h + 1]; p++) {
+        const ulonglong2 b = piece_best[p];
+        if (b.y == ~0ull) continue;
+        if (!has || Hook<A>::better(b.x, best)) {
+          has = true;
+          best = b.x;
+          meta = b.y;
+        }
+      }
+    }
+    const bool upd = h < nh && pull_commit<A>(g, has, v, best, (uint32_t)meta, (uint32_t)(meta >> 32));
+    local += upd;
+    warp_append(upd, v, fout, fout_n, FULL);
+    if (mst) mark_modified(g, upd, v, mst);
+  }
+  warp_add_result(local, &g.ctl[C_RESULT]);
 }
 
 // Bottom-up BFS level for full builds (the reference's dense pull,
@@ -736,7 +851,7 @@ __global__ void k_bfs_bottom_up(DevGraph g, uint32_t *fout, unsigned long long *
         const uint32_t u = P_::nbr(e);
         scanned++;
         if (u & DEAD) continue;
-        if (ld_v32(g.val32, u) == d) {
+        if (__ldca(&g.val32[u]) == d) {  // a stale value only hides a parent found this level
           g.lab[v] = make_ulonglong2(d + 1, pack_parent(u, P_::wt(e)));
           g.val32[v] = (uint32_t)(d + 1);
           found = true;
@@ -749,6 +864,112 @@ __global__ void k_bfs_bottom_up(DevGraph g, uint32_t *fout, unsigned long long *
   }
   warp_add_result(local, &g.ctl[C_RESULT]);
   warp_add_result(scanned, &g.ctl[C_EDGES]);
+}
+
+// ---- small frontiers: several levels in one CTA -----------------------------
+// Incremental repairs and the tail of a build run many levels whose frontier
+// is a handful of vertices; one launch per level would cost more than the
+// work.  k_push_tiny takes a frontier of at most TINY_N vertices and
+// TINY_EDGES out-slots and keeps relaxing level after level inside one CTA
+// (CTA barriers between levels), until the frontier empties or outgrows those
+// limits; the frontier it leaves is in the level's output queue, as after any
+// other level kernel.  Each slot is found by a binary search of the frontier's
+// degree prefix in shared memory.
+constexpr uint32_t TINY_N = 1024;
+constexpr uint64_t TINY_EDGES = 1ull << 20;
+constexpr int TINY_TPB = 1024;
+
+template <int A, bool W>
+__global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_in, unsigned long long *n_in,
+                                                        uint32_t *q_out, unsigned long long *n_out,
+                                                        uint64_t max_levels, uint64_t max_edges, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_TINY) return;
+  using P_ = PoolT<W>;
+  using Scan = cub::BlockScan<uint32_t, TINY_TPB>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ uint32_t s_pref[TINY_N + 1];
+  __shared__ uint32_t s_v[TINY_N];
+  __shared__ uint64_t s_off[TINY_N];
+  __shared__ uint32_t s_su[TINY_N];
+  __shared__ int s_go;
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.out.pool);
+  unsigned long long *c = g.ctl;
+  const unsigned tid = threadIdx.x;
+  uint32_t *cur = q_in, *nxt = q_out;
+  unsigned long long *cur_n = n_in, *nxt_n = n_out;
+  unsigned long long local = 0, scanned = 0;
+  for (bool first = true;; first = false) {
+    const uint64_t n = *cur_n;
+    // stage the frontier and its degree prefix
+    uint32_t d = 0;
+    if (n <= TINY_N && tid < n) {
+      const uint32_t u = cur[tid];
+      s_v[tid] = u;
+      s_off[tid] = g.out.off[u];
+      s_su[tid] = (uint32_t)ld_v32(g.val32, u);
+      d = seg_len(g.out, u);
+    }
+    uint32_t excl, total;
+    Scan(scan_tmp).ExclusiveSum(d, excl, total);
+    if (tid < TINY_N) s_pref[tid] = excl;
+    if (tid == 0) {
+      s_pref[TINY_N] = total;
+      bool go = n > 0 && n <= TINY_N && total <= max_edges;
+      if (!first && go) {
+        // a new level: the bookkeeping k_level_begin does for the first one
+        const uint64_t lvl = c[C_LEVEL];
+        go = lvl < max_levels;
+        if (go) {
+          c[C_STAMP] += 1;
+          c[C_DEPTH] = lvl;
+          if (lvl < TRACE_CAP) g.trace[lvl] = n;
+          c[C_LEVEL] = lvl + 1;
+          *nxt_n = 0;
+        }
+      }
+      s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    const uint32_t st = (uint32_t)c[C_STAMP];
+    for (uint32_t base = 0; base < total; base += TINY_TPB) {
+      const uint32_t e = base + tid;
+      bool upd = false;
+      uint32_t v = 0;
+      if (e < total) {
+        uint32_t lo = 0, hi = (uint32_t)n - 1;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) >> 1;
+          if (s_pref[mid] <= e) lo = mid;
+          else hi = mid - 1;
+        }
+        const typename P_::E ent = __ldg(&pool[s_off[lo] + (e - s_pref[lo])]);
+        v = P_::nbr(ent);
+        scanned++;
+        if (!(v & DEAD)) upd = relax<A>(g, s_v[lo], s_su[lo], v, P_::wt(ent));
+      }
+      local += upd;
+      const bool app = upd && atomicExch(&g.stamp[v], st) != st;
+      warp_append(app, v, nxt, nxt_n, FULL);
+      if (mst) mark_modified(g, upd, v, mst);
+    }
+    __syncthreads();  // the next level reads the queue this one wrote
+    uint32_t *t = cur;
+    cur = nxt;
+    nxt = t;
+    unsigned long long *tn = cur_n;
+    cur_n = nxt_n;
+    nxt_n = tn;
+  }
+  // leave the frontier in the output queue of the level the launch stands for
+  if (cur != q_out) {
+    const uint64_t n = *cur_n;
+    for (uint64_t i = tid; i < n; i += TINY_TPB) q_out[i] = cur[i];
+    __syncthreads();
+    if (tid == 0) *n_out = n;
+  }
+  warp_add_result(local, &c[C_RESULT]);
+  warp_add_result(scanned, &c[C_EDGES]);
 }
 
 // ---- device-driven level loop ------------------------------------------------
@@ -782,10 +1003,11 @@ __global__ void k_prologue(DevGraph g, unsigned long long inv_tag) { prologue_ct
 __host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
   switch (mode) {
     case M_SPARSE: return 2;
-    case M_PULL: return 1;
+    case M_PULL: return 2;
     case M_DENSE_PUSH: return 2;
     case M_BOTTOM_UP: return 1;
     case M_LBS: return 5;
+    case M_TINY: return 1;
   }
   return 0;
 }
@@ -793,7 +1015,9 @@ __host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
 struct LevelCfg {
   uint64_t dense_div;
   uint64_t lbs_min;
-  uint64_t bu_div;  // BFS builds go bottom-up once frontier * bu_div >= |V|
+  uint64_t bu_div;    // BFS builds go bottom-up once frontier * bu_div >= |V|
+  uint64_t pull_div;  // builds pull once frontier * pull_div >= |V|
+  uint64_t tiny_edges;
   int allow_pull;
   int bottom_up;
 };
@@ -801,10 +1025,25 @@ struct LevelCfg {
 // Picks the level mode from the frontier size (the reference's push/pull rule
 // at core/graph.hpp:334 and its vertex/edge-centric rule at :595-612 play the
 // same role); inside a graph it also selects the SWITCH case to run.
-__global__ void k_level_begin(DevGraph g, const unsigned long long *fin_n, unsigned long long *fout_n, LevelCfg cfg,
-                              int use_switch, cudaGraphConditionalHandle sw) {
+constexpr int LVB_TPB = 256;  // threads of k_level_begin (they sum small frontiers' degrees)
+
+__global__ void __launch_bounds__(LVB_TPB) k_level_begin(DevGraph g, const uint32_t *fin,
+                                                         const unsigned long long *fin_n, unsigned long long *fout_n,
+                                                         LevelCfg cfg, int use_switch, cudaGraphConditionalHandle sw) {
+  __shared__ unsigned long long s_edges;
+  const uint64_t n0 = *fin_n;
+  if (threadIdx.x == 0) s_edges = 0;
+  __syncthreads();
+  if (cfg.tiny_edges && n0 && n0 <= TINY_N) {
+    unsigned long long d = 0;
+    for (uint64_t i = threadIdx.x; i < n0; i += LVB_TPB) d += seg_len(g.out, fin[i]);
+    if (d) atomicAdd(&s_edges, d);
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const bool tiny = cfg.tiny_edges && n0 && n0 <= TINY_N && s_edges <= cfg.tiny_edges;
   unsigned long long *c = g.ctl;
-  const uint64_t n = *fin_n;
+  const uint64_t n = n0;
   const uint64_t lvl = c[C_LEVEL];
   *fout_n = 0;
   c[C_HUBN] = 0;
@@ -814,7 +1053,11 @@ __global__ void k_level_begin(DevGraph g, const unsigned long long *fin_n, unsig
   unsigned long long mode = M_SPARSE;
   if (n == 0) mode = M_EMPTY;
   else if (cfg.bottom_up && n * cfg.bu_div >= g.V) mode = M_BOTTOM_UP;
-  else if (dense && cfg.allow_pull) mode = M_PULL;
+  // pull once the frontier passes |V| / pull_div, and keep pulling until it
+  // falls below 4x that (the frontier's first large levels are hub-heavy, its
+  // last ones are not: the direction switch of Beamer et al., by vertex count)
+  else if (cfg.allow_pull && n * (c[C_MODE] == M_PULL ? (cfg.pull_div + 3) / 4 : cfg.pull_div) >= g.V) mode = M_PULL;
+  else if (tiny) mode = M_TINY;
   else if (dense) mode = M_DENSE_PUSH;
   else if (n >= cfg.lbs_min) mode = M_LBS;
   if (mode == M_DENSE_PUSH) c[C_ACT] += 1;
@@ -1286,22 +1529,123 @@ int guard_counters(Graph &g) {
   return RG_OK;
 }
 
-// In-edge partition for dense pull levels, rebuilt only after the adjacency changed.
-// Dense build levels pull for WCC by default (measured faster there; push wins
-// for BFS / SSSP / SSWP); RG_OPT_DENSE_PULL 0 / 1 force push / pull.
-bool pull_on(const Graph &g, int A) { return g.dense_pull == 1 || (g.dense_pull == 2 && A == RG_WCC); }
+// Sliced-ELL copy of the in-edges for dense pull levels, rebuilt only after
+// the adjacency changed (one degree sort and one copy per version).
+template <bool W>
+int prepare_pull_w(Graph &g) {
+  const uint64_t V = g.V;
+  unsigned long long *cnt = g.sell_cnt;
+  unsigned long long h[2] = {0, 0};
+  auto grow = [&](void **p, uint64_t &cap, uint64_t want, size_t esz) -> int {
+    if (want <= cap && *p) return RG_OK;
+    if (*p) {
+      cudaFree(*p);
+      g.bytes -= cap * esz;
+    }
+    *p = nullptr;
+    cap = 0;
+    const uint64_t c = want + want / 8 + 64;
+    if (cudaMalloc(p, c * esz) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("device allocation failed: pull preparation");
+      return RG_ENOMEM_HBM;
+    }
+    cap = c;
+    g.bytes += c * esz;
+    return RG_OK;
+  };
+  int rc = RG_OK;
+  // 1. hubs and their piece offsets (the hub arrays are sized for every vertex
+  //    once, so their addresses stay fixed for the cached level-loop graph)
+  if ((rc = grow((void **)&g.sell_hub, g.sell_hub_cap, V + 1, 4))) return rc;
+  uint64_t off_cap = g.sell_hub_cap;
+  if (!g.sell_hub_off) {
+    if (cudaMalloc(&g.sell_hub_off, off_cap * 8) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("device allocation failed: pull preparation");
+      return RG_ENOMEM_HBM;
+    }
+    g.bytes += off_cap * 8;
+  }
+  RG_CUDA(cudaMemsetAsync(cnt, 0, 16, g.stream));
+  count_launch(g);
+  k_sell_hubs<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.sell_hub, g.sell_hub_off, cnt);
+  RG_CUDA(cudaMemcpyAsync(h, cnt, 8, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  const uint64_t nh = h[0];
+  RG_CUDA(cudaMemsetAsync(g.sell_hub_off + nh, 0, 8, g.stream));
+  size_t tb = g.cub_tmp_bytes;
+  RG_CUDA(cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.sell_hub_off, g.sell_hub_off, nh + 1, g.stream));
+  uint64_t P = 0;
+  RG_CUDA(cudaMemcpyAsync(&P, g.sell_hub_off + nh, 8, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  const uint64_t n = V + P;
+  // 2. piece table, piece results and row ids
+  if ((rc = grow((void **)&g.sell_piece, g.sell_piece_cap, 3 * (P + 1), 4))) return rc;
+  if ((rc = grow((void **)&g.sell_piece_best, g.sell_best_cap, P + 1, 16))) return rc;
+  if ((rc = grow((void **)&g.sell_row, g.sell_row_cap, n, 4))) return rc;
+  uint32_t *pv = g.sell_piece, *pst = pv + (P + 1), *pln = pst + (P + 1);
+  // 3. keys and ids of all rows (vertices, then pieces), sorted by length
+  uint32_t *key0 = nullptr;
+  void *tmp = nullptr;
+  if (cudaMalloc(&key0, n * 4 * 3 + 64) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("device allocation failed: pull preparation");
+    return RG_ENOMEM_HBM;
+  }
+  uint32_t *id0 = key0 + n, *key1 = id0 + n;
+  count_launch(g, nh ? 2 : 1);
+  k_sell_keys<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, key0, id0);
+  if (nh) k_sell_pieces<<<g.num_sms * 2, TPB, 0, g.stream>>>(g.d, g.sell_hub, g.sell_hub_off, nh, key0, id0, pv, pst, pln);
+  cudaError_t e = cudaGetLastError();
+  tb = 0;
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key0, key1, id0, g.sell_row, (int)n, 0, 32, g.stream);
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, tb + 256);
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairsDescending(tmp, tb, key0, key1, id0, g.sell_row, (int)n, 0, 32, g.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cnt + 1, 0, 8, g.stream);
+  if (e == cudaSuccess) {
+    count_launch(g);
+    k_sell_count<<<g.num_sms * 4, TPB, 0, g.stream>>>(key1, n, cnt + 1);
+    e = cudaMemcpyAsync(h, cnt, 16, cudaMemcpyDeviceToHost, g.stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
+  cudaFree(tmp);
+  const uint64_t rows = h[1], slices = (rows + 31) / 32;
+  // 4. slice offsets
+  uint64_t total = 0;
+  if (e == cudaSuccess) {
+    count_launch(g);
+    k_sell_sizes<<<g.num_sms * 4, TPB, 0, g.stream>>>(key1, slices, g.scratch64);
+    tb = g.cub_tmp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.sell_off, slices + 1, g.stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, g.sell_off + slices, 8, cudaMemcpyDeviceToHost, g.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
+  cudaFree(key0);
+  if (e != cudaSuccess) return cuda_fail(e, "pull preparation");
+  // 5. the entries
+  if ((rc = grow(&g.sell_ent, g.sell_cap, total, W ? 8 : 4))) return rc;
+  count_launch(g);
+  k_sell_fill<W><<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.sell_row, rows, slices, g.sell_off, pv, pst, pln,
+                                                      reinterpret_cast<typename SellE<W>::E *>(g.sell_ent));
+  RG_CUDA(cudaGetLastError());
+  g.sell_hubs = nh;
+  g.sell_rows = rows;
+  g.sell_slices = slices;
+  g.sell_epoch++;
+  g.pull_version = g.adj_version;
+  return RG_OK;
+}
+
+// Dense build levels pull (sliced ELL) for SSSP / SSWP / WCC by default; BFS
+// builds use their bottom-up levels.  RG_OPT_DENSE_PULL 0 / 1 force push / pull.
+bool pull_on(const Graph &g, int A) { return g.dense_pull == 1 || (g.dense_pull == 2 && A != RG_BFS); }
 
 int prepare_pull(Graph &g) {
   if (g.pull_version == g.adj_version) return RG_OK;
-  count_launch(g, 5);
-  k_in_degrees<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.scratch64);
-  size_t tb = g.cub_tmp_bytes;
-  RG_CUDA(cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.pull_P, g.V + 1, g.stream));
-  k_in_base<<<g.num_sms * 8, TPB, 0, g.stream>>>(g.d, g.pull_P, g.pull_base);
-  k_partition_tiles<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.pull_P, g.V, PL_TILE, g.pull_tile);
-  RG_CUDA(cudaGetLastError());
-  g.pull_version = g.adj_version;
-  return RG_OK;
+  return g.weighted ? prepare_pull_w<true>(g) : prepare_pull_w<false>(g);
 }
 
 uint64_t max_levels_of(const Graph &g) { return 4 * (uint64_t)g.V + 1024; }
@@ -1321,11 +1665,19 @@ int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
       k_push_hub<A, W><<<g.num_sms * 8, TPB, 0, s>>>(g.d, g.hubq, hub_n, fout, fout_n, mst);
       break;
     case M_PULL:
-      k_pull_dense<A, W><<<g.num_sms * 3, PL_TPB, 0, s>>>(g.d, g.pull_P, g.pull_base, g.pull_tile, fout, fout_n, mst);
+      k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(
+          g.d, reinterpret_cast<const typename SellE<W>::E *>(g.sell_ent), g.sell_off, g.sell_row, g.sell_rows,
+          g.sell_slices, g.sell_piece_best, fout, fout_n, mst);
+      k_pull_hub_fix<A><<<(unsigned)std::max<uint64_t>(1, (g.sell_hubs + 255) / 256), 256, 0, s>>>(
+          g.d, g.sell_hub, g.sell_hub_off, g.sell_hubs, g.sell_piece_best, fout, fout_n, mst);
       break;
     case M_DENSE_PUSH:
       k_mark_active<<<g.num_sms * 8, TPB, 0, s>>>(g.d, fin, fin_n, g.act);
       k_push_dense<A, W><<<g.num_sms * 3, DN_TPB, 0, s>>>(g.d, g.act, fout, fout_n, mst);
+      break;
+    case M_TINY:
+      k_push_tiny<A, W><<<1, TINY_TPB, 0, s>>>(g.d, g.q[half], fin_n, g.q[half ^ 1], fout_n, max_levels_of(g),
+                                               std::min<uint64_t>(g.tiny_edges, TINY_EDGES), mst);
       break;
     case M_BOTTOM_UP:
       k_bfs_bottom_up<W><<<g.num_sms * 8, TPB, 0, s>>>(g.d, fout, fout_n);
@@ -1343,6 +1695,16 @@ int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
   return cudaGetLastError() == cudaSuccess ? RG_OK : RG_ECUDA;
 }
 
+// Hash of every level-mode knob: cached graphs bake them into kernel arguments.
+uint64_t cfg_key(const LevelCfg &c) {
+  uint64_t h = splitmix64(c.dense_div);
+  h = splitmix64(h ^ c.lbs_min);
+  h = splitmix64(h ^ c.bu_div);
+  h = splitmix64(h ^ c.pull_div);
+  h = splitmix64(h ^ c.tiny_edges);
+  return splitmix64(h ^ ((uint64_t)c.allow_pull << 1) ^ (uint64_t)c.bottom_up);
+}
+
 LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   LevelCfg cfg;
   cfg.dense_div = g.dense_div;
@@ -1350,6 +1712,8 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   cfg.allow_pull = (build_variant && pull_on(g, A)) ? 1 : 0;
   cfg.bottom_up = (A == RG_BFS && build_variant && g.bfs_bottom_up) ? 1 : 0;
   cfg.bu_div = g.bu_div;
+  cfg.pull_div = g.pull_div;
+  cfg.tiny_edges = g.tiny_edges < TINY_EDGES ? g.tiny_edges : TINY_EDGES;
   return cfg;
 }
 
@@ -1384,15 +1748,17 @@ int add_level_loop(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
     for (int half = 0; half < 2 && e == cudaSuccess && !rc; half++) {
       cudaGraphConditionalHandle sw;
       if ((e = cudaGraphConditionalHandleCreate(&sw, body, 0, 0)) != cudaSuccess) break;
+      const uint32_t *fin = g.q[half];
       const unsigned long long *fin_n = &g.d.ctl[C_QN0 + half];
       unsigned long long *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
       int use_switch = 1;
       LevelCfg c = cfg;
-      void *args[] = {(void *)&g.d, (void *)&fin_n, (void *)&fout_n, (void *)&c, (void *)&use_switch, (void *)&sw};
+      void *args[] = {(void *)&g.d, (void *)&fin, (void *)&fin_n, (void *)&fout_n, (void *)&c, (void *)&use_switch,
+                      (void *)&sw};
       cudaKernelNodeParams kp = {};
       kp.func = (void *)k_level_begin;
       kp.gridDim = dim3(1);
-      kp.blockDim = dim3(1);
+      kp.blockDim = dim3(LVB_TPB);
       kp.kernelParams = args;
       cudaGraphNode_t kn;
       if ((e = cudaGraphAddKernelNode(&kn, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp)) != cudaSuccess) break;
@@ -1498,8 +1864,7 @@ template <int A, bool W>
 int loop_exec(Graph &g, bool build_variant, cudaGraphExec_t *out) {
   const LevelCfg cfg = level_cfg(g, A, build_variant);
   LoopGraph &slot = g.loops[(A * 2 + (W ? 1 : 0)) * 2 + (build_variant ? 1 : 0)];
-  const uint64_t key = (g.layout_version << 40) ^ (cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^ (cfg.bu_div << 28) ^
-                       ((uint64_t)cfg.allow_pull << 1) ^ (uint64_t)cfg.bottom_up;
+  const uint64_t key = cfg_key(cfg) ^ splitmix64(g.layout_version) ^ splitmix64(build_variant ? g.sell_epoch + 5 : 0);
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
     return RG_OK;
@@ -1553,8 +1918,8 @@ int push_levels(Graph &g, bool build_variant) {
     }
     RG_CUDA(cudaEventRecord(g.pev[0], g.stream));
     count_launch(g);
-    k_level_begin<<<1, 1, 0, g.stream>>>(g.d, &g.d.ctl[C_QN0 + half], &g.d.ctl[C_QN0 + (half ^ 1)], cfg, 0,
-                                          cudaGraphConditionalHandle{});
+    k_level_begin<<<1, LVB_TPB, 0, g.stream>>>(g.d, g.q[half], &g.d.ctl[C_QN0 + half], &g.d.ctl[C_QN0 + (half ^ 1)],
+                                                cfg, 0, cudaGraphConditionalHandle{});
     if ((rc = read_ctl(g))) return rc;
     const unsigned long long mode = g.h_ctl[C_MODE];
     count_launch(g, mode_launches(mode));
@@ -1731,9 +2096,8 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.lb_P, V * 8 + 16, "frontier degree prefix"))) return rc;
   if ((rc = alloc((void **)&g.act, V * 4 + 4, "dense-level activity"))) return rc;
   if ((rc = alloc((void **)&g.lb_sums, SC_BLOCKS * 8, "scan block sums"))) return rc;
-  if ((rc = alloc((void **)&g.pull_P, V * 8 + 16, "in-degree prefix"))) return rc;
-  if ((rc = alloc((void **)&g.pull_base, V * 8 + 8, "in-segment bases"))) return rc;
-  if ((rc = alloc((void **)&g.pull_tile, (g.d.in.pool_cap / PL_TILE + 4) * 4, "pull partition"))) return rc;
+  if ((rc = alloc((void **)&g.sell_off, (V / 32 + 4) * 8, "pull slice offsets"))) return rc;
+  if ((rc = alloc((void **)&g.sell_cnt, 16, "pull counters"))) return rc;
   RG_CUDA(cudaMemset(g.act, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.lb_tile, (g.d.out.pool_cap / LB_TILE + 4) * 4, "tile partition"))) return rc;
   g.cub_tmp_bytes = 0;
@@ -1806,7 +2170,7 @@ int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
   const LevelCfg cfg = level_cfg(g, A, false);
   const uint64_t key = splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
                        splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^
-                       splitmix64((cfg.lbs_min << 20) ^ (cfg.dense_div << 2) ^ 3) ^
+                       cfg_key(cfg) ^
                        splitmix64(recompute_threshold(g) + 11);
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
