@@ -761,9 +761,9 @@ __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename
       // Source values through L1: the values of popular sources stay there.
       // A value cached before its owner improved in this level is only older,
       // and that owner is in the next frontier anyway.
-      uint64_t sv[N];
+      uint32_t sv[N];  // every hook's values fit 32 bits
 #pragma unroll
-      for (int k = 0; k < N; k++) sv[k] = S_::nbr(e[k]) != NONE ? (uint64_t)__ldca(&g.val32[S_::nbr(e[k])]) : 0;
+      for (int k = 0; k < N; k++) sv[k] = S_::nbr(e[k]) != NONE ? __ldca(&g.val32[S_::nbr(e[k])]) : 0u;
 #pragma unroll
       for (int k = 0; k < N; k++) {
         if (S_::nbr(e[k]) == NONE) continue;
