@@ -62,6 +62,10 @@ def parse():
     ap.add_argument("--served-scale", type=int, default=24, help="RMAT scale of the served instance (0 = skip)")
     ap.add_argument("--served-seconds", type=float, default=1.0, help="load duration per client count")
     ap.add_argument("--think-us", type=float, default=50.0, help="mean exponential think time per client")
+    ap.add_argument("--batch-sweep", action="store_true",
+                    help="only the batched incremental sweep (SSSP and SSWP, batches 1..100k) on RMAT-<served-scale>")
+    ap.add_argument("--served-mix", action="store_true",
+                    help="only the six-instance served mix (RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC)")
     return ap.parse_args()
 
 
@@ -261,8 +265,117 @@ def served_leg(args):
     return out
 
 
+def batch_sweep(args):
+    """Batched incremental SSSP / SSWP: the first 90% of an RMAT graph loaded,
+    then sliding-window batches of 1 .. 100,000 insert+delete pairs through
+    rg_apply_add_pairs / rg_apply_del_pairs (host buffers in); pairs/s and the
+    per-batch latency, then incremental == rebuild."""
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    scale = args.served_scale
+    pairs = gen.rmat(scale, seed=args.seed)
+    V = 1 << scale
+    E = len(pairs)
+    imported = int(E * 0.9)
+    root = gen.max_out_degree_vertex(pairs, V)
+    out = {"workload": f"batched incremental sliding window, RMAT-{scale}, first 90% loaded", "runs": []}
+    for algo in ("sssp", "sswp"):
+        g = rg.Graph(V, E, weighted=True)
+        g.add_pairs(pairs[:imported], True, want_old=False)
+        g.build_tree(algo, root)
+        lo = imported
+        for b in (1, 10, 100, 1000, 10000, 100000):
+            nb = int(min(4000, max(20, 3e6 // b)))
+            ts = []
+            for _ in range(nb):
+                if lo + b > E:
+                    break
+                t0 = time.perf_counter()
+                g.apply_add_pairs(algo, pairs[lo:lo + b])
+                g.apply_del_pairs(algo, pairs[lo - imported:lo - imported + b])
+                ts.append(time.perf_counter() - t0)
+                lo += b
+            ts = np.array(ts)
+            out["runs"].append({"algo": algo, "batch": b, "batches": len(ts),
+                                "pairs_per_s": 2 * b * len(ts) / float(ts.sum()),
+                                "p50_ms": float(np.percentile(ts, 50)) * 1e3,
+                                "p99_ms": float(np.percentile(ts, 99)) * 1e3})
+        inc = g.values()
+        g.build_tree(algo, root)
+        out[f"{algo}_incremental_equals_rebuild"] = bool(np.array_equal(inc, g.values()))
+        g.close()
+    return out
+
+
+def served_mix(args):
+    """Six resident instances of uneven size (RMAT 24 SSSP, 23 BFS, 22 WCC,
+    20 SSSP, 18 BFS, 16 WCC), admitted against an HBM budget, served together;
+    closed-loop clients (exponential think time) split evenly, doubled until
+    p99 passes 1 ms; the batched server against the per-update path."""
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    spec = [(24, "sssp"), (23, "bfs"), (22, "wcc"), (20, "sssp"), (18, "bfs"), (16, "wcc")]
+    insts = []
+    for scale, algo in spec:
+        pairs = gen.rmat(scale, seed=scale)
+        V = 1 << scale
+        imported = int(len(pairs) * 0.9)
+        root = gen.max_out_degree_vertex(pairs, V)
+        g = rg.Graph(V, len(pairs), symmetric=algo == "wcc", dual=algo != "wcc", weighted=algo == "sssp")
+        g.add_pairs(pairs[:imported], algo != "wcc", want_old=False)
+        g.build_tree(algo, root)
+        insts.append(dict(scale=scale, algo=algo, pairs=pairs, imported=imported, g=g, root=root, offset=0))
+    dev = sum(i["g"].device_bytes() for i in insts)
+    out = {"workload": "six instances RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC, sliding windows, "
+                       f"closed-loop clients, think {args.think_us:g} us", "device_bytes": dev}
+    for mode, per_update in (("per_update", True), ("served", False)):
+        sweep, best = [], None
+        with rg.Server(hbm_budget_bytes=int(dev * 1.05), per_update=per_update, max_epoch=1 << 16,
+                       target_epoch_ms=0.4) as srv:
+            ids = [srv.attach(i["g"], directed=i["algo"] != "wcc") for i in insts]
+            per = 1
+            while per <= 1024:
+                loads = [dict(instance=k, clients=per, pairs=i["pairs"], imported=i["imported"],
+                              duration_s=args.served_seconds, think_us=args.think_us, weighted=i["algo"] == "sssp",
+                              offset=i["offset"], seed=per) for k, i in zip(ids, insts)]
+                res = srv.run_load(loads)
+                st = srv.stats(reset=True)
+                for i, r in zip(insts, res):
+                    i["offset"] += r["adds"] + r["dels"]
+                pt = {"clients": 6 * per, "updates_per_s": sum(r["updates_per_s"] for r in res),
+                      "p50_us": st["p50_us"], "p99_us": st["p99_us"], "p999_us": st["p999_us"],
+                      "per_instance_updates_per_s": [r["updates_per_s"] for r in res]}
+                sweep.append(pt)
+                if st["p99_us"] <= 1000.0 and (best is None or pt["updates_per_s"] > best["updates_per_s"]):
+                    best = pt
+                if st["p99_us"] > 1000.0 and per >= 4:
+                    break
+                per *= 2
+            for k in ids:
+                srv.detach(k)
+        out[mode] = {"best_at_p99_le_1ms": best, "sweep": sweep}
+    ok = True
+    for i in insts:
+        inc = i["g"].values()
+        i["g"].build_tree(i["algo"], i["root"])
+        ok &= bool(np.array_equal(inc, i["g"].values()))
+        i["g"].close()
+    out["incremental_equals_rebuild"] = ok
+    b0, b1 = out["per_update"]["best_at_p99_le_1ms"], out["served"]["best_at_p99_le_1ms"]
+    out["served_over_per_update"] = (b1["updates_per_s"] / b0["updates_per_s"]) if b0 and b1 else None
+    return out
+
+
 def main():
     args = parse()
+    if args.batch_sweep or args.served_mix:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if int(os.environ.get("RANK", "0")) == 0:
+            res = batch_sweep(args) if args.batch_sweep else served_mix(args)
+            print(json.dumps({"metric": METRIC, "mode": "batch_sweep" if args.batch_sweep else "served_mix",
+                              "data": "synthetic", **res}))
+        return
     if args.impl == "reference":
         return run_reference(args)
     import torch

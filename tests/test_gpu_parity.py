@@ -100,6 +100,38 @@ def test_inc_single_updates_vs_oracle(algo):
     np.testing.assert_array_equal(val, og.labels()[0])
 
 
+def test_bfs_inc_rmat16_10k_steps():
+    """Plain incremental BFS at its headline size: RMAT-16 (65,536 vertices,
+    1,048,576 edges), the first 90% loaded, root 0, then 10,000 sliding-window
+    steps (insert raw[i], delete raw[i - imported]), each repaired at once;
+    the depth of every vertex is compared after every step through the
+    value checksum: against the reference-built driver when it is present,
+    and against the oracle port."""
+    scale, steps = 16, 10000
+    pairs = gen.rmat(scale, seed=16)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    g = gpu_graph("bfs", V, pairs[:imported], hint=len(pairs), inc_mode=True)
+    og = oracle_graph("bfs", V, pairs[:imported], inc_mode=True)
+    g.build_tree("bfs", 0)
+    og.build_tree(0)
+    ref = og.run_inc(pairs, imported, steps, 0)
+    assert len(ref) == steps
+    from oracle import oracle as O
+    if O.ref_available():
+        _, arrays = O.ref_run("inc", "bfs", pairs, V, 0, 0.9, steps)
+        np.testing.assert_array_equal(arrays["sums"][:steps], ref)
+    sums = np.zeros(steps, np.uint64)
+    for k in range(steps):
+        i = imported + k
+        g.apply_add_pairs("bfs", pairs[i:i + 1], True)
+        g.apply_del_pairs("bfs", pairs[k:k + 1], True)
+        sums[k] = g.checksum()
+    np.testing.assert_array_equal(sums, ref)
+    val = check_tree(g, og)
+    np.testing.assert_array_equal(val, og.labels()[0])
+
+
 @pytest.mark.parametrize("algo", ALGOS)
 def test_reference_api_sequence(algo):
     """The driver sequence with host decisions (src/sssp_inc.cpp:295-324):
