@@ -107,6 +107,12 @@ int rg_classify(rg_graph *g, int algo, const rg_edge *edges, const uint8_t *is_d
 int rg_apply_add(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int directed, uint64_t *old_num);
 int rg_apply_del(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int directed, uint64_t *old_num);
 
+/* One step of src/sssp_inc_batch.cpp:141-175: rg_apply_add of `adds`, then
+ * rg_apply_del of `dels`, as one device submission with one synchronisation
+ * when both batches hold at most 2048 edges (two submissions otherwise). */
+int rg_apply_add_del(rg_graph *g, int algo, const rg_edge *adds, uint64_t n_add, const rg_edge *dels, uint64_t n_del,
+                     int directed);
+
 /* rg_apply_add / rg_apply_del over reference-format pairs (see rg_add_pairs). */
 int rg_apply_add_pairs(rg_graph *g, int algo, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num);
 int rg_apply_del_pairs(rg_graph *g, int algo, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num);

@@ -84,6 +84,7 @@ def _declare(L):
         "rg_classify": [P, _int, P, P, _u64, _int, P],
         "rg_apply_add": [P, _int, P, _u64, _int, P],
         "rg_apply_del": [P, _int, P, _u64, _int, P],
+        "rg_apply_add_del": [P, _int, P, _u64, P, _u64, _int],
         "rg_apply_add_pairs": [P, _int, P, _u64, _int, P],
         "rg_apply_del_pairs": [P, _int, P, _u64, _int, P],
         "rg_get_labels": [P, P, P, P],
@@ -302,6 +303,13 @@ class Graph:
 
     def apply_del(self, algo: str, edges, directed: bool = True) -> np.ndarray:
         return self._apply(lib().rg_apply_del, algo, as_edges(edges), directed, "rg_apply_del")
+
+    def apply_add_del(self, algo: str, adds, dels, directed: bool = True):
+        """rg_apply_add of `adds` then rg_apply_del of `dels` in one submission."""
+        a, d = as_edges(adds), as_edges(dels)
+        _check(lib().rg_apply_add_del(self._h, ALGOS[algo], _p(a), len(a), _p(d), len(d), int(directed)),
+               "rg_apply_add_del")
+        self.algo = algo
 
     def apply_add_pairs(self, algo: str, pairs, directed: bool = True, want_old: bool = False):
         p = np.ascontiguousarray(pairs, dtype=np.uint64).reshape(-1)

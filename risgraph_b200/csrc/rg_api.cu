@@ -207,6 +207,10 @@ int rg_destroy(rg_graph *gh) {
     if (l.exec) cudaGraphExecDestroy(l.exec);
   for (auto &l : g.dels)
     if (l.exec) cudaGraphExecDestroy(l.exec);
+  for (auto &l : g.applies)
+    if (l.exec) cudaGraphExecDestroy(l.exec);
+  for (auto &l : g.mixes)
+    if (l.exec) cudaGraphExecDestroy(l.exec);
   if (g.cap_stream) cudaStreamDestroy(g.cap_stream);
   cudaFree(g.d.trace);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
@@ -244,6 +248,19 @@ int rg_apply_del(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int di
   int rc = check_graph(g);
   if (!rc) rc = check_algo(g->g, algo);
   return rc ? rc : edge_updates(g, edges, nullptr, n, directed, old_num, false, true);
+}
+
+int rg_apply_add_del(rg_graph *g, int algo, const rg_edge *adds, uint64_t n_add, const rg_edge *dels, uint64_t n_del,
+                     int directed) {
+  int rc = check_graph(g);
+  if (!rc) rc = check_algo(g->g, algo);
+  if (!rc) rc = check_edges(g->g, adds, nullptr, n_add);
+  if (!rc) rc = check_edges(g->g, dels, nullptr, n_del);
+  if (rc) return rc;
+  if (n_add && n_del && n_add <= rg::SMALL_EDGES && n_del <= rg::SMALL_EDGES && !g->g.profiling)
+    return rg::apply_add_del_small(g->g, adds, n_add, dels, n_del, directed);
+  rc = edge_updates(g, adds, nullptr, n_add, directed, nullptr, true, true);
+  return rc ? rc : edge_updates(g, dels, nullptr, n_del, directed, nullptr, false, true);
 }
 
 int rg_apply_add_pairs(rg_graph *g, int algo, const uint64_t *pairs, uint64_t n, int directed, uint64_t *old_num) {

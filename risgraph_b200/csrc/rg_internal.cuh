@@ -207,17 +207,21 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t *q, 
 }
 
 // Header of a small update batch in the graph's mapped pinned staging buffer,
-// read by the fused apply kernel; the edges follow at APPLY_DATA_OFF and the
-// per-edge old counts are written back at apply_old_off(cap).
+// read by the fused apply kernel.  A submission holds up to two headers (an
+// insert batch at offset 0, a delete batch at APPLY_HDR2); the edges follow at
+// APPLY_DATA_OFF + data_off, and the per-edge old counts of a single batch are
+// written back at apply_old_off().
 struct ApplyHdr {
   uint64_t n;         // edges in the batch
   uint64_t pairs;     // 1: reference-format (src,dst) pairs, 0: rg_edge records
   uint64_t inv_tag;   // invalidation tag of a deletion repair
   uint64_t want_old;  // 1: write the old counts back
+  uint64_t data_off;  // offset of the batch's edges from APPLY_DATA_OFF
 };
-constexpr uint64_t APPLY_DATA_OFF = 64;
+constexpr uint64_t APPLY_HDR2 = 64;
+constexpr uint64_t APPLY_DATA_OFF = 128;
 constexpr uint64_t SMALL_EDGES = 2048;  // largest batch of the fused single-CTA apply path
-inline uint64_t apply_old_off() { return APPLY_DATA_OFF + SMALL_EDGES * sizeof(rg_edge); }
+inline uint64_t apply_old_off() { return APPLY_DATA_OFF + 2 * SMALL_EDGES * sizeof(rg_edge); }
 
 // A cached, instantiated level-loop graph.
 struct LoopGraph {
@@ -284,8 +288,9 @@ struct Graph {
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
   LoopGraph loops[16];
   LoopGraph dels[8];
-  // fused small-batch apply graphs: [algo][weighted][add][directed]
+  // fused small-batch apply graphs: [algo][weighted][add][directed]; insert+delete pairs: [algo][weighted][directed]
   LoopGraph applies[32];
+  LoopGraph mixes[16];
   cudaStream_t cap_stream = nullptr;
   uint64_t layout_version = 1;  // bumped when pool buffers move (compaction)
   void *cub_tmp = nullptr;
@@ -366,6 +371,11 @@ int tree_alloc(Graph &g);
 // conditional node, one graph launch and one synchronisation in all.
 int apply_small(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
                 uint64_t *old_num);
+// An insert batch and a delete batch (each <= SMALL_EDGES) in one graph launch:
+// the two fused applies back to back, the delete one skipped if the insert
+// one stopped on a storage error.
+int apply_add_del_small(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge *dels, uint64_t n_del,
+                        int directed);
 
 }  // namespace rg
 

@@ -10,9 +10,9 @@
 // Here every instance owns a worker thread and the graph's own CUDA stream.
 // The worker takes everything that queued while its previous epoch was on the
 // GPU (up to an adaptive cap) and applies it as one add batch and one delete
-// batch through the fused storage + repair submission (rg_apply_add /
-// rg_apply_del): safe updates cost only their multiplicity change, unsafe ones
-// share one repair.  Batching changes no result: the values after an epoch are
+// batch through the fused storage + repair submission (rg_apply_add_del, one
+// launch for both when they are small): safe updates cost only their
+// multiplicity change, unsafe ones share one repair.  Batching changes no result: the values after an epoch are
 // the unique fixpoint of the graph after the epoch's updates.  The one order
 // that batching could change, a delete of an edge followed by an insert of the
 // same edge (adds run before deletes), ends the epoch before the insert.
@@ -140,8 +140,12 @@ void worker_main(rg_server *s, Instance *in) {
     for (const Item &it : batch) (it.r.type ? dels : adds).push_back(rg_edge{it.r.src, it.r.dst, it.r.data});
     const uint64_t t0 = now_ns();
     int rc = RG_OK;
-    if (!adds.empty()) rc = rg_apply_add(in->g, in->algo, adds.data(), adds.size(), in->directed, nullptr);
-    if (!rc && !dels.empty()) rc = rg_apply_del(in->g, in->algo, dels.data(), dels.size(), in->directed, nullptr);
+    if (!adds.empty() && !dels.empty())
+      rc = rg_apply_add_del(in->g, in->algo, adds.data(), adds.size(), dels.data(), dels.size(), in->directed);
+    else if (!adds.empty())
+      rc = rg_apply_add(in->g, in->algo, adds.data(), adds.size(), in->directed, nullptr);
+    else if (!dels.empty())
+      rc = rg_apply_del(in->g, in->algo, dels.data(), dels.size(), in->directed, nullptr);
     const uint64_t t1 = now_ns();
     // Adapt the cap to keep one epoch within the target (cf. the threshold
     // update of src/sssp_inc_rt.cpp:394-412, driven by time instead of timeouts).

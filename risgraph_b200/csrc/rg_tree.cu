@@ -1217,23 +1217,37 @@ constexpr int FS_TPB = 1024;
 
 template <int A, bool W>
 __global__ void __launch_bounds__(FS_TPB)
-    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const void *data, uint64_t *old_host,
-                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, cudaGraphConditionalHandle repair) {
+    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data_base, uint64_t *old_host,
+                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
+                  cudaGraphConditionalHandle repair) {
   __shared__ sdev::GrowShared gsh;
-  __shared__ uint64_t s_n, s_pairs, s_want;
+  __shared__ uint64_t s_n, s_pairs, s_want, s_off;
+  __shared__ int s_skip;
   unsigned long long *c = g.ctl;
   const unsigned tid = threadIdx.x;
   if (tid == 0) {
-    // the host wrote the header before the launch; read it past any cache
-    s_n = __ldcv(&hdr->n);
-    s_pairs = __ldcv(&hdr->pairs);
-    s_want = __ldcv(&hdr->want_old);
-    prologue_ctl(c, __ldcv(&hdr->inv_tag));
-    c[C_CANDN] = 0;
-    c[C_GROWN_OUT] = 0;
-    c[C_GROWN_IN] = 0;
+    // the second batch of a submission does nothing after an error in the first
+    s_skip = second && c[C_ERR] != 0;
+    if (!s_skip) {
+      // the host wrote the header before the launch; read it past any cache
+      s_n = __ldcv(&hdr->n);
+      s_pairs = __ldcv(&hdr->pairs);
+      s_want = __ldcv(&hdr->want_old);
+      s_off = __ldcv(&hdr->data_off);
+      const unsigned long long kl = c[C_KLAUNCH];
+      prologue_ctl(c, __ldcv(&hdr->inv_tag));
+      if (second) c[C_KLAUNCH] = kl;  // the count covers the whole submission
+      c[C_CANDN] = 0;
+      c[C_GROWN_OUT] = 0;
+      c[C_GROWN_IN] = 0;
+    }
   }
   __syncthreads();
+  if (s_skip) {
+    if (tid == 0) cudaGraphSetConditional(repair, 0u);
+    return;
+  }
+  const void *data = data_base + s_off;
   const uint64_t n = s_n < SMALL_EDGES ? s_n : SMALL_EDGES;
   const uint64_t nops = directed ? n : 2 * n;
   const int weighted = W ? 1 : 0;
@@ -2160,6 +2174,96 @@ int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t
   return rc;
 }
 
+// One fused apply phase as graph nodes: k_apply_small (reading the header at
+// hdr_off of the staging buffer) -> IF (frontier) { [deletion repair ->] level
+// loop }.  *out is the IF node.
+template <int A, bool W>
+int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps,
+                    cudaGraphConditionalHandle ih, bool add, int directed, uint64_t hdr_off, int second,
+                    const LevelCfg &cfg, cudaGraphNode_t *out) {
+  sdev::OpView ops = sdev::op_view(g);
+  char *base = reinterpret_cast<char *>(g.stage_host_dev);
+  const ApplyHdr *hdr = reinterpret_cast<const ApplyHdr *>(base + hdr_off);
+  const char *data = base + APPLY_DATA_OFF;
+  uint64_t *old_host = reinterpret_cast<uint64_t *>(base + apply_old_off());
+  uint32_t *cand = op_cand(g);
+  int a_add = add ? 1 : 0, a_dir = directed ? 1 : 0, a_second = second;
+  uint32_t *q0 = g.q[0];
+  uint32_t mst = mod_stamp(g);
+  void *args[] = {(void *)&g.d,  (void *)&ops, (void *)&hdr, (void *)&data,     (void *)&old_host, (void *)&cand,
+                  (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&a_second, (void *)&ih};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void *)k_apply_small<A, W>;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(FS_TPB);
+  kp.kernelParams = args;
+  cudaGraphNode_t kn;
+  cudaError_t e = cudaGraphAddKernelNode(&kn, graph, deps, ndeps, &kp);
+  if (e != cudaSuccess) return cuda_fail(e, "building the fused apply graph");
+  cudaGraphNodeParams ip = {};
+  ip.type = cudaGraphNodeTypeConditional;
+  ip.conditional.handle = ih;
+  ip.conditional.type = cudaGraphCondTypeIf;
+  ip.conditional.size = 1;
+  if ((e = cudaGraphAddNode(out, graph, &kn, 1, &ip)) != cudaSuccess) return cuda_fail(e, "building the fused apply graph");
+  cudaGraph_t body = ip.conditional.phGraph_out[0];
+  cudaGraphNode_t last, loop;
+  if (add) return add_level_loop<A, W>(g, body, nullptr, 0, cfg, &loop);
+  int rc = add_del_repair<A, W>(g, body, nullptr, 0, &last);
+  if (!rc) rc = add_level_loop<A, W>(g, body, &last, 1, cfg, &loop);
+  return rc;
+}
+
+uint64_t apply_key(const Graph &g, const LevelCfg &cfg) {
+  return splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
+         splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^ cfg_key(cfg) ^ splitmix64(recompute_threshold(g) + 11);
+}
+
+// Insert batch then delete batch in one graph: phase 1 (header 1) -> phase 2
+// (header 2, skipped after an error in phase 1) -> control block to the host.
+template <int A, bool W>
+int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
+  LoopGraph &slot = g.mixes[(A * 2 + (W ? 1 : 0)) * 2 + (directed ? 1 : 0)];
+  const LevelCfg cfg = level_cfg(g, A, false);
+  const uint64_t key = apply_key(g, cfg);
+  if (slot.exec && slot.key == key) {
+    *out = slot.exec;
+    return RG_OK;
+  }
+  if (slot.exec) {
+    cudaGraphExecDestroy(slot.exec);
+    slot.exec = nullptr;
+  }
+  cudaGraph_t graph;
+  RG_CUDA(cudaGraphCreate(&graph, 0));
+  int rc = RG_OK;
+  cudaError_t e = cudaSuccess;
+  do {
+    cudaGraphConditionalHandle h1, h2;
+    if ((e = cudaGraphConditionalHandleCreate(&h1, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    if ((e = cudaGraphConditionalHandleCreate(&h2, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    cudaGraphNode_t if1, if2, mn;
+    if ((rc = add_apply_phase<A, W>(g, graph, nullptr, 0, h1, true, directed, 0, 0, cfg, &if1))) break;
+    if ((rc = add_apply_phase<A, W>(g, graph, &if1, 1, h2, false, directed, APPLY_HDR2, 1, cfg, &if2))) break;
+    if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &if2, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
+                                      cudaMemcpyDeviceToHost)) != cudaSuccess)
+      break;
+    e = cudaGraphInstantiate(&slot.exec, graph, 0);
+  } while (0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    slot.exec = nullptr;
+    return cuda_fail(e, "building the fused insert+delete graph");
+  }
+  if (rc) {
+    slot.exec = nullptr;
+    return rc;
+  }
+  slot.key = key;
+  *out = slot.exec;
+  return RG_OK;
+}
+
 // Fused small-batch apply graph per (algorithm, weighting, add/delete,
 // directed): k_apply_small -> IF (frontier) { [deletion repair ->] level loop }
 // -> control block to the host.  Its parameters hold the op, staging and pool
@@ -2168,10 +2272,7 @@ template <int A, bool W>
 int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
   LoopGraph &slot = g.applies[((A * 2 + (W ? 1 : 0)) * 2 + (add ? 1 : 0)) * 2 + (directed ? 1 : 0)];
   const LevelCfg cfg = level_cfg(g, A, false);
-  const uint64_t key = splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
-                       splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^
-                       cfg_key(cfg) ^
-                       splitmix64(recompute_threshold(g) + 11);
+  const uint64_t key = apply_key(g, cfg);
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
     return RG_OK;
@@ -2187,40 +2288,8 @@ int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
   do {
     cudaGraphConditionalHandle ih;
     if ((e = cudaGraphConditionalHandleCreate(&ih, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    sdev::OpView ops = sdev::op_view(g);
-    char *base = reinterpret_cast<char *>(g.stage_host_dev);
-    const ApplyHdr *hdr = reinterpret_cast<const ApplyHdr *>(base);
-    const void *data = base + APPLY_DATA_OFF;
-    uint64_t *old_host = reinterpret_cast<uint64_t *>(base + apply_old_off());
-    uint32_t *cand = op_cand(g);
-    int a_add = add ? 1 : 0, a_dir = directed ? 1 : 0;
-    uint32_t *q0 = g.q[0];
-    uint32_t mst = mod_stamp(g);
-    void *args[] = {(void *)&g.d, (void *)&ops, (void *)&hdr, (void *)&data, (void *)&old_host, (void *)&cand,
-                    (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&ih};
-    cudaKernelNodeParams kp = {};
-    kp.func = (void *)k_apply_small<A, W>;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(FS_TPB);
-    kp.kernelParams = args;
-    cudaGraphNode_t kn;
-    if ((e = cudaGraphAddKernelNode(&kn, graph, nullptr, 0, &kp)) != cudaSuccess) break;
-    cudaGraphNodeParams ip = {};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = ih;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
     cudaGraphNode_t ifn;
-    if ((e = cudaGraphAddNode(&ifn, graph, &kn, 1, &ip)) != cudaSuccess) break;
-    cudaGraph_t body = ip.conditional.phGraph_out[0];
-    cudaGraphNode_t last, loop;
-    if (add) {
-      rc = add_level_loop<A, W>(g, body, nullptr, 0, cfg, &loop);
-    } else {
-      rc = add_del_repair<A, W>(g, body, nullptr, 0, &last);
-      if (!rc) rc = add_level_loop<A, W>(g, body, &last, 1, cfg, &loop);
-    }
-    if (rc) break;
+    if ((rc = add_apply_phase<A, W>(g, graph, nullptr, 0, ih, add, directed, 0, 0, cfg, &ifn))) break;
     cudaGraphNode_t mn;
     if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &ifn, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
                                       cudaMemcpyDeviceToHost)) != cudaSuccess)
@@ -2244,7 +2313,7 @@ int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
 template <int A, bool W>
 int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
                   uint64_t *old_num) {
-  int rc = storage_reserve(g, 2 * SMALL_EDGES);  // op arrays and staging sized once for the small path
+  int rc = storage_reserve(g, 3 * SMALL_EDGES);  // op arrays and staging sized once for the small path
   if (rc) return rc;
   char *st = reinterpret_cast<char *>(g.stage_host);
   ApplyHdr *h = reinterpret_cast<ApplyHdr *>(st);
@@ -2254,6 +2323,7 @@ int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_
   h->pairs = pairs ? 1 : 0;
   h->want_old = old_num ? 1 : 0;
   h->inv_tag = 0;
+  h->data_off = 0;
   g.adj_version++;
   if ((rc = guard_counters(g))) return rc;
   if (!add) {
@@ -2287,6 +2357,64 @@ int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_
   if (old_num) std::memcpy(old_num, replayed ? (const void *)storage_old_host(g) : (const void *)(st + apply_old_off()),
                            n * 8);
   return RG_OK;
+}
+
+template <int A, bool W>
+int apply_add_del_t(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge *dels, uint64_t n_del,
+                    int directed) {
+  int rc = storage_reserve(g, 3 * SMALL_EDGES);
+  if (rc) return rc;
+  char *st = reinterpret_cast<char *>(g.stage_host);
+  ApplyHdr *h1 = reinterpret_cast<ApplyHdr *>(st), *h2 = reinterpret_cast<ApplyHdr *>(st + APPLY_HDR2);
+  std::memcpy(st + APPLY_DATA_OFF, adds, n_add * sizeof(rg_edge));
+  std::memcpy(st + APPLY_DATA_OFF + n_add * sizeof(rg_edge), dels, n_del * sizeof(rg_edge));
+  *h1 = ApplyHdr{n_add, 0, 0, 0, 0};
+  *h2 = ApplyHdr{n_del, 0, 0, 0, n_add * sizeof(rg_edge)};
+  g.adj_version++;
+  if ((rc = guard_counters(g))) return rc;
+  if (++g.inv_epoch >= 0x7FFFFFFFu) {
+    RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+    g.inv_epoch = 1;
+  }
+  h2->inv_tag = 2ull * g.inv_epoch;
+  reset_stats(g);
+  cudaGraphExec_t exec;
+  if ((rc = mixed_exec<A, W>(g, directed, &exec))) return rc;
+  count_launch(g, 2);
+  RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  if (g.h_ctl[C_ERR] == RG_ENOSPACE && g.h_ctl[C_AUX] == 1) {
+    // the insert phase ran out of pool during growth (the delete phase did not
+    // run): compact, replay the inserts, then apply the deletes on their own
+    const uint64_t nops = directed ? n_add : 2 * n_add;
+    rc = storage_recover(g);
+    if (!rc) rc = storage_replay(g, n_add, nops, directed, true);
+    if (!rc) rc = dispatch(g, A, 1, n_add, directed, true, 0);
+    if (!rc) rc = sync_ctl(g);
+    if (!rc) rc = storage_error(g);
+    if (!rc) rc = after_sync<A, W>(g, 1);
+    if (rc) return rc;
+    return n_del ? apply_small_t<A, W>(g, dels, nullptr, n_del, directed, false, nullptr) : RG_OK;
+  }
+  if ((rc = storage_error(g))) return rc;
+  return after_sync<A, W>(g, 2);
+}
+
+int apply_add_del_small(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge *dels, uint64_t n_del,
+                        int directed) {
+  const bool W = g.weighted != 0;
+  switch (g.algo) {
+    case RG_BFS: return W ? apply_add_del_t<RG_BFS, true>(g, adds, n_add, dels, n_del, directed)
+                          : apply_add_del_t<RG_BFS, false>(g, adds, n_add, dels, n_del, directed);
+    case RG_SSSP: return W ? apply_add_del_t<RG_SSSP, true>(g, adds, n_add, dels, n_del, directed)
+                           : apply_add_del_t<RG_SSSP, false>(g, adds, n_add, dels, n_del, directed);
+    case RG_SSWP: return W ? apply_add_del_t<RG_SSWP, true>(g, adds, n_add, dels, n_del, directed)
+                           : apply_add_del_t<RG_SSWP, false>(g, adds, n_add, dels, n_del, directed);
+    case RG_WCC: return W ? apply_add_del_t<RG_WCC, true>(g, adds, n_add, dels, n_del, directed)
+                          : apply_add_del_t<RG_WCC, false>(g, adds, n_add, dels, n_del, directed);
+  }
+  set_error("labels were not built (call rg_build_tree first)");
+  return RG_ESTATE;
 }
 
 int apply_small(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,

@@ -366,3 +366,30 @@ def test_pool_exhaustion_is_a_status():
     with pytest.raises(rg.RGError) as ei:
         g.add_pairs(pairs, want_old=False)
     assert ei.value.status == 5
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("batch", [1, 37, 2048, 3000])
+def test_apply_add_del_one_submission(algo, batch):
+    """rg_apply_add_del (inserts then deletes of a sliding-window batch, one
+    device submission up to 2048 + 2048 edges) gives the oracle's values after
+    every batch."""
+    scale = 12
+    pairs = gen.rmat(scale, seed=31)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    nb = 6 if batch < 2048 else 2
+    g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs), inc_mode=True)
+    og = oracle_graph(algo, V, pairs[:imported], inc_mode=True)
+    g.build_tree(algo, 0)
+    og.build_tree(0)
+    ref = og.run_batch(pairs, imported, batch, nb, 0)
+    directed = algo != "wcc"
+    for k in range(len(ref)):
+        lo = imported + k * batch
+        hi = min(lo + batch, len(pairs))
+        adds = edges_of(algo, pairs[lo:hi])
+        dels = edges_of(algo, pairs[lo - imported:hi - imported])
+        g.apply_add_del(algo, adds, dels, directed)
+        assert g.checksum() == int(ref[k]), f"batch {k}"
+    check_tree(g, og)
