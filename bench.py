@@ -66,6 +66,10 @@ def parse():
                     help="only the batched incremental sweep (SSSP and SSWP, batches 1..100k) on RMAT-<served-scale>")
     ap.add_argument("--served-mix", action="store_true",
                     help="only the six-instance served mix (RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC)")
+    ap.add_argument("--wcc-deletions", action="store_true",
+                    help="only incremental WCC with heavy deletion on an ER+RMAT mix of 2^wcc-scale vertices")
+    ap.add_argument("--wcc-scale", type=int, default=26)
+    ap.add_argument("--wcc-updates", type=int, default=1000000)
     return ap.parse_args()
 
 
@@ -366,8 +370,81 @@ def served_mix(args):
     return out
 
 
+def wcc_deletions(args):
+    """Incremental WCC with heavy deletion: an undirected graph of 2^s vertices
+    and 16 * 2^s edges (half uniform endpoints, half RMAT-s), both directions
+    stored; the first 80% loaded; then batches of 1,000 updates (500 inserts of
+    the next edges, 500 deletes of which half remove the oldest loaded edges and
+    half remove current tree edges (a vertex's parent edge), forcing subtree
+    repair), each batch one rg_apply_add_del; min-vertex-id labels checked
+    against a rebuild at the end."""
+    import ctypes
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    scale = args.wcc_scale
+    V = 1 << scale
+    E = 16 * V
+    t0 = time.time()
+    pairs = gen.er_rmat_mix(scale, E, seed=args.seed)
+    imported = int(E * 0.8)
+    g = rg.Graph(V, E, symmetric=True, dual=False, weighted=False)
+    g.add_pairs(pairs[:imported], directed=False, want_old=False)
+    load_s = time.time() - t0
+    t1 = time.time()
+    g.build_tree("wcc", 0)
+    build_ms = (time.time() - t1) * 1e3
+    rng = np.random.default_rng(args.seed)
+    par = np.empty(V, np.uint64)
+    L = rg.lib()
+
+    def refresh():
+        assert L.rg_get_labels(g._h, None, ctypes.c_void_p(par.ctypes.data), None) == 0
+        return np.nonzero(par != V)[0]
+
+    batch, half = 1000, 500
+    nb = min(args.wcc_updates // batch, (E - imported) // half)
+    ts, recomputes, invalidated = [], 0, 0
+    have = refresh()
+    for k in range(nb):
+        if k % 50 == 0 and k:
+            have = refresh()
+        lo = imported + k * half
+        adds = pairs[lo:lo + half]
+        old = pairs[k * (half // 2):(k + 1) * (half // 2)]
+        vs = rng.choice(have, half // 2, replace=False) if len(have) >= half // 2 else have
+        tree = np.stack([par[vs], vs.astype(np.uint64)], axis=1)
+        dels = np.concatenate([old, tree]).astype(np.uint64)
+        t = time.perf_counter()
+        g.apply_add_del("wcc", adds, dels, directed=False)
+        ts.append(time.perf_counter() - t)
+        st = g.last_stats()
+        recomputes += st["recomputes"]
+        invalidated += st["invalidated"]
+    ts = np.array(ts)
+    inc = g.values()
+    g.build_tree("wcc", 0)
+    ok = bool(np.array_equal(inc, g.values()))
+    out = {"workload": f"incremental WCC, ER+RMAT mix: 2^{scale} vertices, {E} undirected edges (half uniform, "
+                       f"half RMAT-{scale}) stored both ways, first 80% loaded, {nb} batches of {batch} updates "
+                       f"(500 inserts, 250 oldest-edge deletes, 250 tree-edge deletes)",
+           "device_bytes": g.device_bytes(), "load_s": load_s, "build_ms": build_ms, "batches": int(nb),
+           "updates_per_s": batch * nb / float(ts.sum()) if nb else None,
+           "batch_p50_ms": float(np.percentile(ts, 50)) * 1e3 if nb else None,
+           "batch_p99_ms": float(np.percentile(ts, 99)) * 1e3 if nb else None,
+           "invalidated_per_batch": invalidated / max(nb, 1), "full_recomputes": recomputes,
+           "incremental_equals_rebuild": ok}
+    g.close()
+    return out
+
+
 def main():
     args = parse()
+    if args.wcc_deletions:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"metric": METRIC, "mode": "wcc_deletions", "data": "synthetic", **wcc_deletions(args)}))
+        return
     if args.batch_sweep or args.served_mix:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))

@@ -267,6 +267,7 @@ struct Graph {
   void *sell_ent = nullptr;       // entries, slice-major, column-major inside a slice
   uint64_t sell_cap = 0;          // entries allocated
   uint64_t *sell_off = nullptr;   // slice offsets (entries), slices + 1
+  uint64_t sell_off_cap = 0;
   uint32_t *sell_row = nullptr;   // row ids by length, descending: vertex id, or |V| + hub piece index
   uint64_t sell_row_cap = 0;
   uint32_t *sell_hub = nullptr;   // hub vertices (in-list longer than a row)

@@ -1627,8 +1627,12 @@ int prepare_pull_w(Graph &g) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
   cudaFree(tmp);
   const uint64_t rows = h[1], slices = (rows + 31) / 32;
-  // 4. slice offsets
+  // 4. slice offsets (rows count hub pieces too, so there can be more than |V|)
   uint64_t total = 0;
+  if (e == cudaSuccess && (rc = grow((void **)&g.sell_off, g.sell_off_cap, slices + 1, 8))) {
+    cudaFree(key0);
+    return rc;
+  }
   if (e == cudaSuccess) {
     count_launch(g);
     k_sell_sizes<<<g.num_sms * 4, TPB, 0, g.stream>>>(key1, slices, g.scratch64);
@@ -2110,7 +2114,6 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.lb_P, V * 8 + 16, "frontier degree prefix"))) return rc;
   if ((rc = alloc((void **)&g.act, V * 4 + 4, "dense-level activity"))) return rc;
   if ((rc = alloc((void **)&g.lb_sums, SC_BLOCKS * 8, "scan block sums"))) return rc;
-  if ((rc = alloc((void **)&g.sell_off, (V / 32 + 4) * 8, "pull slice offsets"))) return rc;
   if ((rc = alloc((void **)&g.sell_cnt, 16, "pull counters"))) return rc;
   RG_CUDA(cudaMemset(g.act, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.lb_tile, (g.d.out.pool_cap / LB_TILE + 4) * 4, "tile partition"))) return rc;

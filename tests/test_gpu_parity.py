@@ -41,6 +41,23 @@ def test_build_tree_parity(algo, scale):
     np.testing.assert_array_equal(g.values(), val)
 
 
+@pytest.mark.parametrize("algo", ALGOS)
+def test_build_tree_parity_er_rmat_mix(algo):
+    """Half uniform, half RMAT endpoints: nearly every vertex has in-edges and
+    the RMAT hubs are cut into several pull pieces, so the sliced in-edge copy
+    has more rows than vertices."""
+    scale = 14
+    V = 1 << scale
+    pairs = gen.er_rmat_mix(scale, 64 * V, seed=5)
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = gpu_graph(algo, V, pairs)
+    og = oracle_graph(algo, V, pairs)
+    g.build_tree(algo, root)
+    og.build_tree(root)
+    val = check_tree(g, og, root)
+    np.testing.assert_array_equal(val, og.labels()[0])
+
+
 @pytest.mark.parametrize("name", [n for n in json.load(open(os.path.join(GOLDEN, "index.json")))])
 def test_golden_reference_fixtures(name):
     """Against values and per-step checksums produced by the reference itself."""
