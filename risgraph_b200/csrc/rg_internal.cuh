@@ -279,6 +279,7 @@ struct Graph {
   uint64_t sell_best_cap = 0;
   unsigned long long *sell_cnt = nullptr;
   uint64_t sell_hubs = 0, sell_rows = 0, sell_slices = 0, sell_epoch = 0;
+  uint64_t sell_cls[3] = {0, 0, 0};  // first slice of width <= 8, 4, 2
   uint64_t pull_div = 64;
   uint64_t tiny_edges = 32768;  // frontiers with at most this many out-slots run in k_push_tiny (0: off)
   uint64_t adj_version = 1, pull_version = 0;

@@ -720,19 +720,100 @@ __device__ __forceinline__ bool pull_commit(const DevGraph &g, bool has, uint32_
   return true;
 }
 
+// Commit of one pulled row (all lanes of the warp call it).
+template <int A>
+__device__ __forceinline__ void pull_row_done(const DevGraph &g, bool active, uint32_t id, bool has, uint64_t best,
+                                              uint32_t bsrc, uint32_t bw, ulonglong2 *piece_best, uint32_t *fout,
+                                              unsigned long long *fout_n, uint32_t mst, unsigned long long &local) {
+  bool upd = false;
+  if (active && id < g.V) {
+    upd = pull_commit<A>(g, has, id, best, bsrc, bw);
+  } else if (active) {
+    // a hub piece: its best waits for k_pull_hub_fix
+    piece_best[id - g.V] = make_ulonglong2(best, has ? pack_parent(bsrc, bw) : ~0ull);
+  }
+  local += upd;
+  warp_append(upd, id, fout, fout_n, FULL);
+  if (mst) mark_modified(g, upd, id, mst);
+}
+
+template <int A, bool W>
+__device__ __forceinline__ void pull_take(const typename SellE<W>::E &e, uint32_t sv, bool &has, uint64_t &best,
+                                          uint32_t &bsrc, uint32_t &bw) {
+  using S_ = SellE<W>;
+  if (S_::nbr(e) == NONE) return;
+  const uint64_t c = Hook<A>::combine(sv, S_::wt(e));
+  if (!has || Hook<A>::better(c, best)) {
+    has = true;
+    best = c;
+    bsrc = S_::nbr(e);
+    bw = S_::wt(e);
+  }
+}
+
+// Source values through L1: the values of popular sources stay there.  A value
+// cached before its owner improved in this level is only older, and that owner
+// is in the next frontier anyway.
+__device__ __forceinline__ uint32_t pull_src_val(const DevGraph &g, uint32_t u) {
+  return u != NONE ? __ldca(&g.val32[u]) : 0u;
+}
+
+// Slices are sorted by width (the length of their longest row).  Wide slices
+// (more than 8 entries per row) take a warp each and stream their rows 16 (or
+// 8 + 8 prefetched) entries at a time; narrower slices are taken G at a time
+// (G = 2, 4, 8 for widths up to 8, 4, 2) so that every lane still keeps 16
+// entries in flight per round trip.  cls[0..2]: first slice of width <= 8, 4, 2.
+struct PullClasses {
+  uint64_t c8, c4, c2;
+};
+
+template <int A, bool W, int G>
+__device__ __forceinline__ void pull_narrow(const DevGraph &g, const typename SellE<W>::E *ent, const uint64_t *off,
+                                            const uint32_t *row_id, uint64_t rows, uint64_t lo, uint64_t hi,
+                                            ulonglong2 *piece_best, uint32_t *fout, unsigned long long *fout_n,
+                                            uint32_t mst, unsigned long long &local, uint64_t warp, uint64_t nwarps) {
+  using S_ = SellE<W>;
+  constexpr int NP = 16 / G;
+  const int lane = lane_id();
+  for (uint64_t s0 = lo + warp * G; s0 < hi; s0 += nwarps * G) {
+    typename S_::E e[16];
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      const uint64_t s = s0 + gi;
+      const uint64_t o = s < hi ? off[s] : 0, w = s < hi ? (off[s + 1] - o) >> 5 : 0;
+#pragma unroll
+      for (int k = 0; k < NP; k++) e[gi * NP + k] = k < w ? __ldcs(&ent[o + (uint64_t)k * 32 + lane]) : S_::none();
+    }
+    uint32_t sv[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) sv[k] = pull_src_val(g, S_::nbr(e[k]));
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      const uint64_t s = s0 + gi;
+      const uint64_t r = s * 32 + lane;
+      const bool active = s < hi && r < rows;
+      bool has = false;
+      uint64_t best = 0;
+      uint32_t bsrc = 0, bw = 0;
+#pragma unroll
+      for (int k = 0; k < NP; k++) pull_take<A, W>(e[gi * NP + k], sv[gi * NP + k], has, best, bsrc, bw);
+      pull_row_done<A>(g, active, active ? row_id[r] : 0u, has, best, bsrc, bw, piece_best, fout, fout_n, mst, local);
+    }
+  }
+}
+
 template <int A, bool W>
 __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename SellE<W>::E *ent, const uint64_t *off,
                                                       const uint32_t *row_id, uint64_t rows, uint64_t slices,
-                                                      ulonglong2 *piece_best, uint32_t *fout,
+                                                      PullClasses cls, ulonglong2 *piece_best, uint32_t *fout,
                                                       unsigned long long *fout_n, uint32_t mst) {
   if (g.ctl[C_MODE] != M_PULL) return;
   using S_ = SellE<W>;
   const int lane = lane_id();
-  const uint64_t V = g.V;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long local = 0;
-  for (uint64_t s = warp; s < slices; s += nwarps) {
+  for (uint64_t s = warp; s < cls.c8; s += nwarps) {
     const uint64_t r = s * 32 + lane;
     const bool active = r < rows;
     const uint32_t id = active ? row_id[r] : 0u;
@@ -758,37 +839,30 @@ __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename
           e[k] = j + k < width ? __ldcs(&col[(j + k) * 32]) : S_::none();
         }
       }
-      // Source values through L1: the values of popular sources stay there.
-      // A value cached before its owner improved in this level is only older,
-      // and that owner is in the next frontier anyway.
       uint32_t sv[N];  // every hook's values fit 32 bits
 #pragma unroll
-      for (int k = 0; k < N; k++) sv[k] = S_::nbr(e[k]) != NONE ? __ldca(&g.val32[S_::nbr(e[k])]) : 0u;
+      for (int k = 0; k < N; k++) sv[k] = pull_src_val(g, S_::nbr(e[k]));
 #pragma unroll
-      for (int k = 0; k < N; k++) {
-        if (S_::nbr(e[k]) == NONE) continue;
-        const uint64_t c = Hook<A>::combine(sv[k], S_::wt(e[k]));
-        if (!has || Hook<A>::better(c, best)) {
-          has = true;
-          best = c;
-          bsrc = S_::nbr(e[k]);
-          bw = S_::wt(e[k]);
-        }
-      }
+      for (int k = 0; k < N; k++) pull_take<A, W>(e[k], sv[k], has, best, bsrc, bw);
     }
-    bool upd = false;
-    if (active && id < V) {
-      upd = pull_commit<A>(g, has, id, best, bsrc, bw);
-    } else if (active) {
-      // a hub piece: its best waits for k_pull_hub_fix
-      piece_best[id - V] = make_ulonglong2(best, has ? pack_parent(bsrc, bw) : ~0ull);
-    }
-    local += upd;
-    warp_append(upd, id, fout, fout_n, FULL);
-    if (mst) mark_modified(g, upd, id, mst);
+    pull_row_done<A>(g, active, id, has, best, bsrc, bw, piece_best, fout, fout_n, mst, local);
   }
+  pull_narrow<A, W, 2>(g, ent, off, row_id, rows, cls.c8, cls.c4, piece_best, fout, fout_n, mst, local, warp, nwarps);
+  pull_narrow<A, W, 4>(g, ent, off, row_id, rows, cls.c4, cls.c2, piece_best, fout, fout_n, mst, local, warp, nwarps);
+  pull_narrow<A, W, 8>(g, ent, off, row_id, rows, cls.c2, slices, piece_best, fout, fout_n, mst, local, warp, nwarps);
   warp_add_result(local, &g.ctl[C_RESULT]);
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&g.ctl[C_EDGES], off[slices]);
+}
+
+// First slice whose width is at most 8, 4, 2 (slice widths never increase).
+__global__ void k_sell_classes(const uint32_t *sorted_key, uint64_t slices, unsigned long long *cls) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < slices; s += stride) {
+    const uint32_t w = sorted_key[s * 32], wp = s ? sorted_key[(s - 1) * 32] : 0xFFFFFFFFu;
+    if (w <= 8 && wp > 8) cls[0] = s;
+    if (w <= 4 && wp > 4) cls[1] = s;
+    if (w <= 2 && wp > 2) cls[2] = s;
+  }
 }
 
 // One warp per hub: best of its pieces, one write.
@@ -1640,6 +1714,13 @@ int prepare_pull_w(Graph &g) {
     e = cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.sell_off, slices + 1, g.stream);
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(&total, g.sell_off + slices, 8, cudaMemcpyDeviceToHost, g.stream);
+  unsigned long long cls[3] = {slices, slices, slices};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g.sell_cnt + 2, cls, 24, cudaMemcpyHostToDevice, g.stream);
+  if (e == cudaSuccess) {
+    count_launch(g);
+    k_sell_classes<<<g.num_sms * 4, TPB, 0, g.stream>>>(key1, slices, g.sell_cnt + 2);
+    e = cudaMemcpyAsync(cls, g.sell_cnt + 2, 24, cudaMemcpyDeviceToHost, g.stream);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
   cudaFree(key0);
   if (e != cudaSuccess) return cuda_fail(e, "pull preparation");
@@ -1652,6 +1733,10 @@ int prepare_pull_w(Graph &g) {
   g.sell_hubs = nh;
   g.sell_rows = rows;
   g.sell_slices = slices;
+  // classes are nested: a slice of width <= 2 is also <= 4 and <= 8
+  g.sell_cls[2] = cls[2];
+  g.sell_cls[1] = std::min<uint64_t>(cls[1], g.sell_cls[2]);
+  g.sell_cls[0] = std::min<uint64_t>(cls[0], g.sell_cls[1]);
   g.sell_epoch++;
   g.pull_version = g.adj_version;
   return RG_OK;
@@ -1685,7 +1770,8 @@ int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
     case M_PULL:
       k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(
           g.d, reinterpret_cast<const typename SellE<W>::E *>(g.sell_ent), g.sell_off, g.sell_row, g.sell_rows,
-          g.sell_slices, g.sell_piece_best, fout, fout_n, mst);
+          g.sell_slices, PullClasses{g.sell_cls[0], g.sell_cls[1], g.sell_cls[2]}, g.sell_piece_best, fout, fout_n,
+          mst);
       k_pull_hub_fix<A><<<(unsigned)std::max<uint64_t>(1, (g.sell_hubs + 255) / 256), 256, 0, s>>>(
           g.d, g.sell_hub, g.sell_hub_off, g.sell_hubs, g.sell_piece_best, fout, fout_n, mst);
       break;
@@ -2114,7 +2200,7 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.lb_P, V * 8 + 16, "frontier degree prefix"))) return rc;
   if ((rc = alloc((void **)&g.act, V * 4 + 4, "dense-level activity"))) return rc;
   if ((rc = alloc((void **)&g.lb_sums, SC_BLOCKS * 8, "scan block sums"))) return rc;
-  if ((rc = alloc((void **)&g.sell_cnt, 16, "pull counters"))) return rc;
+  if ((rc = alloc((void **)&g.sell_cnt, 64, "pull counters"))) return rc;
   RG_CUDA(cudaMemset(g.act, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.lb_tile, (g.d.out.pool_cap / LB_TILE + 4) * 4, "tile partition"))) return rc;
   g.cub_tmp_bytes = 0;
