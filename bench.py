@@ -269,6 +269,24 @@ def served_leg(args):
     return out
 
 
+def max_over_ranks(x, dist):
+    """The slowest rank's time (every rank takes part; NCCL ranks reduce on
+    their GPU, gloo ranks on the CPU)."""
+    if not dist:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, world, seconds):
+    """Whole-job GTEPS of `world` independent replicas, each processing
+    units_per_rank edges, timed by the slowest rank."""
+    return units_per_rank * world / seconds / 1e9
+
+
 def batch_sweep(args):
     """Batched incremental SSSP / SSWP: the first 90% of an RMAT graph loaded,
     then sliding-window batches of 1 .. 100,000 insert+delete pairs through
@@ -497,11 +515,8 @@ def main():
     launches = g.launch_count() - l0
     times = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(times))
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = E_r * args.steps * world / (total_ms / 1e3) / 1e9
+    total_ms = max_over_ranks(total_ms, dist)
+    value = replica_throughput(E_r * args.steps, world, total_ms / 1e3)
 
     # end to end through the API: build + value readback into pinned memory
     host_vals = torch.empty(V, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
@@ -516,12 +531,9 @@ def main():
         rc = L.rg_get_labels(g._h, ctypes.c_void_p(host_vals.ctypes.data), None, None)
         assert rc == 0
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     assert np.array_equal(host_vals, values)
-    e2e = E_r * args.steps * world / e2e_s / 1e9
+    e2e = replica_throughput(E_r * args.steps, world, e2e_s)
 
     # roofline of the level-relaxation kernels (k_push + k_push_hub)
     g.profile(True)
