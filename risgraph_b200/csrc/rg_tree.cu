@@ -1397,16 +1397,12 @@ __device__ __forceinline__ bool has_parents(const DevGraph &g, uint32_t x, uint3
 // in-neighbour satisfies equal_func and has a clean parent chain; the parent
 // moves to that in-edge.  One warp per frontier vertex.
 template <int A, bool W>
-__global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
-                                                uint64_t limit) {
-  if (g.ctl[C_RECOMPUTE]) return;
+__device__ __forceinline__ void rescue_warps(const DevGraph &g, const uint32_t *fin, uint64_t n, uint64_t limit,
+                                             uint64_t warp, uint64_t nwarps) {
   const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
-  const uint64_t n = *fin_n;
   const int lane = lane_id();
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t idx = warp; idx < n; idx += nwarps) {
     const uint32_t d = fin[idx];
     if (ld_u32(&g.inv[d]) != tag_inv) continue;
@@ -1441,19 +1437,25 @@ __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin,
   }
 }
 
+template <int A, bool W>
+__global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
+                                                uint64_t limit) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  rescue_warps<A, W>(g, fin, *fin_n, limit, warp, nwarps);
+}
+
 // Collect and expand (core/graph.hpp:1363-1417): a still-invalid vertex joins
 // the reset set; its tree children (parent == (u,w)) are invalidated next.
 template <int A, bool W>
-__global__ void __launch_bounds__(TPB) k_expand(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
-                                                uint32_t *tree, uint32_t *fout, unsigned long long *fout_n) {
-  if (g.ctl[C_RECOMPUTE]) return;
+__device__ __forceinline__ void expand_warps(const DevGraph &g, const uint32_t *fin, uint64_t n, uint32_t *tree,
+                                             uint32_t *fout, unsigned long long *fout_n, uint64_t warp,
+                                             uint64_t nwarps) {
   const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.out.pool);
-  const uint64_t n = *fin_n;
   const int lane = lane_id();
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t idx = warp; idx < n; idx += nwarps) {
     const uint32_t u = fin[idx];
     if (ld_u32(&g.inv[u]) != tag_inv) continue;
@@ -1480,14 +1482,20 @@ __global__ void __launch_bounds__(TPB) k_expand(DevGraph g, const uint32_t *fin,
   }
 }
 
-// Reset the invalid set to init (core/graph.hpp:1420-1430).
-template <int A>
-__global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long long *tree_n, uint32_t mst) {
+template <int A, bool W>
+__global__ void __launch_bounds__(TPB) k_expand(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
+                                                uint32_t *tree, uint32_t *fout, unsigned long long *fout_n) {
   if (g.ctl[C_RECOMPUTE]) return;
-  const uint64_t root = g.ctl[C_ROOT];
-  const uint64_t n = *tree_n;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  expand_warps<A, W>(g, fin, *fin_n, tree, fout, fout_n, warp, nwarps);
+}
+
+// Reset the invalid set to init (core/graph.hpp:1420-1430).
+template <int A>
+__device__ __forceinline__ void reset_warps(const DevGraph &g, const uint32_t *tree, uint64_t n, uint32_t mst,
+                                            uint64_t warp, uint64_t nwarps) {
+  const uint64_t root = g.ctl[C_ROOT];
   for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
     uint64_t i = base + lane_id();
     uint32_t u = 0;
@@ -1500,18 +1508,22 @@ __global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long lo
   }
 }
 
+template <int A>
+__global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long long *tree_n, uint32_t mst) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  reset_warps<A>(g, tree, *tree_n, mst, warp, nwarps);
+}
+
 // One transposed pull over the reset set (core/graph.hpp:1433-1511): each
 // vertex takes its best in-neighbour by update_func.  One warp per vertex.
 template <int A, bool W>
-__global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
-                                              uint32_t mst) {
-  if (g.ctl[C_RECOMPUTE]) return;
+__device__ __forceinline__ unsigned long long pull_warps(const DevGraph &g, const uint32_t *fin, uint64_t n,
+                                                         uint32_t mst, uint64_t warp, uint64_t nwarps) {
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
-  const uint64_t n = *fin_n;
   const int lane = lane_id();
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long local = 0;
   for (uint64_t idx = warp; idx < n; idx += nwarps) {
     const uint32_t d = fin[idx];
@@ -1540,7 +1552,108 @@ __global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, c
     local += upd;
     if (mst) mark_modified(g, __shfl_sync(FULL, upd, 0) && lane == 0, d, mst);
   }
+  return local;
+}
+
+template <int A, bool W>
+__global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, const unsigned long long *fin_n,
+                                              uint32_t mst) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long local = pull_warps<A, W>(g, fin, *fin_n, mst, warp, nwarps);
   warp_add_result(local, &g.ctl[C_RESULT]);
+}
+
+// Small deletion repairs in one CTA: the invalidation levels (rescue, expand),
+// the reset and the pull with CTA barriers in place of launches, then the
+// reset set copied to queue 0 for the push loop.  When a level's frontier or
+// the reset set outgrows one CTA it hands over to the multi-CTA repair (the
+// IF node it opens), with the frontier left in queue 0 where that repair
+// starts.
+constexpr int DT_TPB = 1024;
+constexpr uint64_t DEL_TINY_N = 1024, DEL_TINY_TREE = 8192;
+
+template <int A, bool W>
+__global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, uint32_t *q1, uint32_t *tree,
+                                                     uint64_t limit, uint64_t big, uint64_t max_iter, uint32_t mst,
+                                                     cudaGraphConditionalHandle standard) {
+  __shared__ int s_go;
+  unsigned long long *c = g.ctl;
+  const unsigned tid = threadIdx.x;
+  const uint64_t warp = tid >> 5, nwarps = DT_TPB / 32;
+  uint32_t *cur = q0, *nxt = q1;
+  unsigned long long *cur_n = &c[C_QN0], *nxt_n = &c[C_QN1];
+  for (;;) {
+    if (tid == 0) {
+      const uint64_t n = *cur_n;
+      int go = 1;  // 1: run this level; 0: invalidation done; 2: hand over
+      if (n == 0 || c[C_RECOMPUTE]) {
+        go = 0;
+      } else if (n > DEL_TINY_N) {
+        go = 2;
+      } else {
+        const uint64_t it = c[C_INVITER];
+        if (it >= max_iter) {
+          go = 0;
+        } else if (it <= 10 && c[C_TREEN] + n > big) {  // core/graph.hpp:1252
+          c[C_RECOMPUTE] = 1;
+          go = 0;
+        } else {
+          c[C_INVITER] = it + 1;
+          *nxt_n = 0;
+        }
+      }
+      if (go == 0 && c[C_TREEN] > DEL_TINY_TREE && !c[C_RECOMPUTE]) go = 2;
+      s_go = go;
+    }
+    __syncthreads();
+    if (s_go != 1) break;
+    const uint64_t n = *cur_n;
+    rescue_warps<A, W>(g, cur, n, limit, warp, nwarps);
+    __syncthreads();
+    expand_warps<A, W>(g, cur, n, tree, nxt, nxt_n, warp, nwarps);
+    __syncthreads();
+    uint32_t *t = cur;
+    cur = nxt;
+    nxt = t;
+    unsigned long long *tn = cur_n;
+    cur_n = nxt_n;
+    nxt_n = tn;
+  }
+  if (s_go == 2) {
+    // the multi-CTA repair continues from queue 0
+    if (cur != q0) {
+      const uint64_t n = *cur_n;
+      for (uint64_t i = tid; i < n; i += DT_TPB) q0[i] = cur[i];
+      __syncthreads();
+      if (tid == 0) c[C_QN0] = n;
+    }
+    if (tid == 0) {
+      c[C_KLAUNCH] += 1;
+      cudaGraphSetConditional(standard, 1u);
+    }
+    return;
+  }
+  unsigned long long local = 0;
+  const bool recompute = c[C_RECOMPUTE] != 0;
+  if (!recompute) {
+    const uint64_t tn = c[C_TREEN];
+    reset_warps<A>(g, tree, tn, mst, warp, nwarps);
+    __syncthreads();
+    local = pull_warps<A, W>(g, tree, tn, mst, warp, nwarps);
+    __syncthreads();
+    for (uint64_t i = tid; i < tn; i += DT_TPB) q0[i] = tree[i];
+    __syncthreads();
+    if (tid == 0) c[C_QN0] = tn;
+  } else if (tid == 0) {
+    c[C_QN0] = 0;
+  }
+  warp_add_result(local, &c[C_RESULT]);
+  if (tid == 0) {
+    c[C_KLAUNCH] += 1;
+    cudaGraphSetConditional(standard, 0u);
+  }
 }
 
 // need_update_tree_add (core/graph.hpp:987-1000) / need_update_tree_del
@@ -1903,11 +2016,13 @@ int add_level_loop(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
 
 // Deletion repair as nodes of a CUDA graph (do_update_tree_del,
 // core/graph.hpp:1235-1612):
-//   WHILE (invalidated frontier non-empty and no recompute) {
-//     k_inv_begin ; k_rescue ; k_expand     (queue 0 -> 1)
-//     k_inv_begin ; k_rescue ; k_expand     (queue 1 -> 0)
-//     k_inv_cond }
-//   k_reset ; k_pull ; k_copy_frontier (reset set -> queue 0 for the push loop)
+//   k_del_tiny (small repairs in one CTA) -> IF (it handed over) {
+//     WHILE (invalidated frontier non-empty and no recompute) {
+//       k_inv_begin ; k_rescue ; k_expand     (queue 0 -> 1)
+//       k_inv_begin ; k_rescue ; k_expand     (queue 1 -> 0)
+//       k_inv_cond }
+//     k_reset ; k_pull ; k_copy_frontier (reset set -> queue 0 for the push loop) }
+// *out is the IF node.
 template <int A, bool W>
 int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps, cudaGraphNode_t *out) {
   if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
@@ -1917,6 +2032,28 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
   const int gridw = g.num_sms * 16;
   cudaError_t e = cudaSuccess;
   do {
+    cudaGraphConditionalHandle th;
+    if ((e = cudaGraphConditionalHandleCreate(&th, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    uint32_t *q0 = g.q[0], *q1 = g.q[1], *tr = g.tree;
+    uint64_t max_iter = (uint64_t)g.V + 2;
+    void *ta[] = {(void *)&g.d, (void *)&q0, (void *)&q1, (void *)&tr, (void *)&limit, (void *)&big,
+                  (void *)&max_iter, (void *)&mst, (void *)&th};
+    cudaKernelNodeParams tp = {};
+    tp.func = (void *)k_del_tiny<A, W>;
+    tp.gridDim = dim3(1);
+    tp.blockDim = dim3(DT_TPB);
+    tp.kernelParams = ta;
+    cudaGraphNode_t tn;
+    if ((e = cudaGraphAddKernelNode(&tn, graph, deps, ndeps, &tp)) != cudaSuccess) break;
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = th;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    if ((e = cudaGraphAddNode(out, graph, &tn, 1, &ip)) != cudaSuccess) break;
+    graph = ip.conditional.phGraph_out[0];  // the multi-CTA repair below goes into the IF body
+    deps = nullptr;
+    ndeps = 0;
     cudaGraphConditionalHandle wh;
     if ((e = cudaGraphConditionalHandleCreate(&wh, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
     cudaGraphNodeParams wp = {};
@@ -1940,7 +2077,6 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
     if ((e = cudaStreamEndCapture(g.cap_stream, &body)) != cudaSuccess) break;
     // k_reset -> k_pull -> k_copy_frontier after the loop
     unsigned long long *tree_n = &g.d.ctl[C_TREEN], *q0_n = &g.d.ctl[C_QN0];
-    uint32_t *q0 = g.q[0];
     const uint32_t *tree = g.tree;
     void *ra[] = {(void *)&g.d, (void *)&tree, (void *)&tree_n, (void *)&mst};
     void *ca[] = {(void *)&g.d, (void *)&tree, (void *)&tree_n, (void *)&q0, (void *)&q0_n};
@@ -1956,7 +2092,8 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
     kp.func = (void *)k_copy_frontier;
     kp.gridDim = dim3(g.num_sms * 4);
     kp.kernelParams = ca;
-    e = cudaGraphAddKernelNode(out, graph, &n2, 1, &kp);
+    cudaGraphNode_t n3;
+    e = cudaGraphAddKernelNode(&n3, graph, &n2, 1, &kp);
   } while (0);
   if (e != cudaSuccess) return cuda_fail(e, "building the deletion-repair graph");
   return RG_OK;
