@@ -20,6 +20,9 @@ BIN = os.path.join(PKG, "bin")
 DRIVER = os.path.join(BIN, "rg_driver")
 # the reference's command-line drivers, all served by one binary (argv[0] picks)
 DRIVER_NAMES = [a + m for a in ("bfs", "sssp", "sswp", "wcc") for m in ("", "_inc", "_inc_batch", "_inc_rt")]
+# the reference's text -> binary converters, one binary likewise
+CONVERT = os.path.join(BIN, "rg_convert")
+CONVERT_NAMES = ["convert_to_binary", "convert_to_binary_random", "convert_to_binary_timestamp"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++"
@@ -82,12 +85,17 @@ def build_drivers(verbose: bool = False, force: bool = False) -> str:
     if force or _newer(DRIVER, [src, LIB, os.path.join(INCLUDE, "risgraph_b200.h")]):
         _run([HOST_CXX, "-std=c++17", "-O2", "-fopenmp", "-I" + INCLUDE, src, "-L" + PKG, "-lrisgraph_b200",
               "-Wl,-rpath,$ORIGIN/..", "-o", DRIVER], verbose)
-    for name in DRIVER_NAMES:
-        link = os.path.join(BIN, name)
-        if not os.path.islink(link):
-            if os.path.exists(link):
-                os.remove(link)
-            os.symlink("rg_driver", link)
+    src = os.path.join(PKG, "cli", "rg_convert.cpp")
+    if force or _newer(CONVERT, [src, LIB]):
+        _run([HOST_CXX, "-std=c++17", "-O2", "-I" + INCLUDE, src, "-L" + PKG, "-lrisgraph_b200",
+              "-Wl,-rpath,$ORIGIN/..", "-o", CONVERT], verbose)
+    for target, names in (("rg_driver", DRIVER_NAMES), ("rg_convert", CONVERT_NAMES)):
+        for name in names:
+            link = os.path.join(BIN, name)
+            if not os.path.islink(link):
+                if os.path.exists(link):
+                    os.remove(link)
+                os.symlink(target, link)
     return DRIVER
 
 

@@ -109,3 +109,29 @@ def test_reference_weights_sssp_inc(tmp_path):
         og.add_edge(s, d, (s + d) % 128)
     og.build_tree(root)
     np.testing.assert_array_equal(np.fromfile(out, dtype=np.uint64), og.labels()[0])
+
+
+def test_converters(tmp_path):
+    """convert_to_binary[_random|_timestamp]: text edge lists to the binary
+    format (utils/convert_to_binary*.cpp)."""
+    rng = np.random.default_rng(3)
+    edges = rng.integers(0, 1 << 40, size=(500, 2), dtype=np.uint64)
+    ts = rng.integers(0, 50, size=500, dtype=np.uint64)
+    txt = "\n".join(f"{s} {d}" for s, d in edges.tolist()) + "\n"
+    txt_t = "\n".join(f"{s}\t{d}\t{t}" for (s, d), t in zip(edges.tolist(), ts.tolist()))
+
+    def conv(name, text, env=None):
+        e = dict(os.environ)
+        e.update(env or {})
+        r = subprocess.run([os.path.join(BIN, name)], input=text.encode(), capture_output=True, env=e, timeout=60)
+        assert r.returncode == 0, r.stderr
+        return np.frombuffer(r.stdout, dtype=np.uint64).reshape(-1, 2)
+
+    np.testing.assert_array_equal(conv("convert_to_binary", txt), edges)
+    a = conv("convert_to_binary_random", txt, {"RG_SHUFFLE_SEED": "7"})
+    b = conv("convert_to_binary_random", txt, {"RG_SHUFFLE_SEED": "7"})
+    np.testing.assert_array_equal(a, b)  # seeded: reproducible
+    assert not np.array_equal(a, edges)
+    np.testing.assert_array_equal(np.sort(a.view("u8,u8"), axis=0), np.sort(edges.view("u8,u8"), axis=0))
+    order = sorted(range(500), key=lambda i: (int(ts[i]), int(edges[i, 0]), int(edges[i, 1])))
+    np.testing.assert_array_equal(conv("convert_to_binary_timestamp", txt_t), edges[order])
