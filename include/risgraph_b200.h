@@ -126,6 +126,26 @@ int rg_get_labels(rg_graph *g, uint64_t *value, uint64_t *parent, uint64_t *pare
 int rg_get_modified(rg_graph *g, uint64_t *vids, uint64_t cap, uint64_t *n);
 int rg_clear_modified(rg_graph *g);
 
+/* Versioned label history: the device form of MVVec (core/mvvec.hpp:23-162),
+ * which the _inc_rt drivers fill after every update with the value of each
+ * modified vertex at the update's version (src/sssp_inc_rt.cpp:338-343).
+ * Needs a trace_modified graph.  rg_history_enable reserves capacity_nodes
+ * history nodes (24 bytes each).  rg_history_record stores, at `version`, the
+ * current value of every vertex modified since the last rg_clear_modified (all
+ * vertices when all_vertices, e.g. version 0 right after rg_build_tree), then
+ * clears the modified list; as MVVec::set, a vertex gets a new node only when
+ * its value changed, and a repeated version overwrites.  RG_ENOSPACE when the
+ * pool is full (nodes that fit are kept).  rg_history_get returns each vertex's
+ * value as of `version` (MVVec::get: the newest node at or before it); found[i]
+ * = 0 when the vertex has no node that old.  rg_history_gc(version) drops the
+ * nodes no reader at or after `version` can see (MVVec::gc) and packs the pool. */
+int rg_history_enable(rg_graph *g, uint64_t capacity_nodes);
+int rg_history_record(rg_graph *g, uint64_t version, int all_vertices);
+int rg_history_get(rg_graph *g, const uint64_t *vids, uint64_t n, uint64_t version, uint64_t *values,
+                   uint8_t *found);
+int rg_history_gc(rg_graph *g, uint64_t version);
+int rg_history_nodes(rg_graph *g, uint64_t *used, uint64_t *capacity);
+
 /* Checksum of the value array on the device (same definition as
  * rg_gen_value_checksum), so per-step checks need no label copy. */
 int rg_value_checksum(rg_graph *g, uint64_t *checksum);

@@ -103,6 +103,11 @@ def _declare(L):
         "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
         "rg_set_option": [P, _int, _u64],
         "rg_get_option": [P, _int, P],
+        "rg_history_enable": [P, _u64],
+        "rg_history_record": [P, _u64, _int],
+        "rg_history_get": [P, P, _u64, _u64, P, P],
+        "rg_history_gc": [P, _u64],
+        "rg_history_nodes": [P, P, P],
         "rg_server_create": [_u64, ctypes.c_double, _u64, _int, P],
         "rg_server_attach": [P, P, _int, _int, P],
         "rg_server_detach": [P, ctypes.c_uint32],
@@ -336,6 +341,29 @@ class Graph:
 
     def values(self) -> np.ndarray:
         return self.labels(True, False, False)[0]
+
+    # -- versioned label history (MVVec, core/mvvec.hpp)
+    def history_enable(self, capacity_nodes: int):
+        _check(lib().rg_history_enable(self._h, int(capacity_nodes)), "rg_history_enable")
+
+    def history_record(self, version: int, all_vertices: bool = False):
+        _check(lib().rg_history_record(self._h, int(version), int(all_vertices)), "rg_history_record")
+
+    def history_get(self, vids, version: int):
+        """(values, found) of the vertices as of `version`."""
+        v = np.ascontiguousarray(vids, dtype=np.uint64)
+        out = np.zeros(len(v), np.uint64)
+        found = np.zeros(len(v), np.uint8)
+        _check(lib().rg_history_get(self._h, _p(v), len(v), int(version), _p(out), _p(found)), "rg_history_get")
+        return out, found.astype(bool)
+
+    def history_gc(self, version: int):
+        _check(lib().rg_history_gc(self._h, int(version)), "rg_history_gc")
+
+    def history_nodes(self):
+        u = np.zeros(2, np.uint64)
+        _check(lib().rg_history_nodes(self._h, _p(u[0:1]), _p(u[1:2])), "rg_history_nodes")
+        return int(u[0]), int(u[1])
 
     def checksum(self) -> int:
         c = np.zeros(1, np.uint64)

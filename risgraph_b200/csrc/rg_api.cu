@@ -195,6 +195,7 @@ int rg_destroy(rg_graph *gh) {
   cudaSetDevice(g.device);
   if (g.stream) cudaStreamSynchronize(g.stream);
   rg::storage_free(g);
+  rg::history_free(g);
   cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
   cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp); cudaFree(g.act);
@@ -382,6 +383,41 @@ int rg_clear_modified(rg_graph *gh) {
   unsigned long long ep = g.mod_epoch;
   RG_CUDA(cudaMemcpyAsync(&g.d.ctl[rg::C_MODEPOCH], &ep, 8, cudaMemcpyHostToDevice, g.stream));
   RG_CUDA(cudaStreamSynchronize(g.stream));
+  return RG_OK;
+}
+
+int rg_history_enable(rg_graph *gh, uint64_t capacity_nodes) {
+  int rc = check_graph(gh);
+  return rc ? rc : rg::history_enable(gh->g, capacity_nodes);
+}
+
+int rg_history_record(rg_graph *gh, uint64_t version, int all_vertices) {
+  int rc = check_graph(gh);
+  if (!rc) rc = rg::history_record(gh->g, version, all_vertices);
+  if (!rc) rc = rg_clear_modified(gh);
+  return rc;
+}
+
+int rg_history_get(rg_graph *gh, const uint64_t *vids, uint64_t n, uint64_t version, uint64_t *values,
+                   uint8_t *found) {
+  int rc = check_graph(gh);
+  if (rc) return rc;
+  if (n && (!vids || !values)) {
+    rg::set_error("null array");
+    return RG_EINVAL;
+  }
+  return rg::history_get(gh->g, vids, n, version, values, found);
+}
+
+int rg_history_gc(rg_graph *gh, uint64_t version) {
+  int rc = check_graph(gh);
+  return rc ? rc : rg::history_gc(gh->g, version);
+}
+
+int rg_history_nodes(rg_graph *gh, uint64_t *used, uint64_t *capacity) {
+  if (!gh) return RG_EINVAL;
+  if (used) *used = gh->g.hist_used;
+  if (capacity) *capacity = gh->g.hist_cap;
   return RG_OK;
 }
 

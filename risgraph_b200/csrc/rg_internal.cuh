@@ -223,6 +223,13 @@ constexpr uint64_t APPLY_DATA_OFF = 128;
 constexpr uint64_t SMALL_EDGES = 2048;  // largest batch of the fused single-CTA apply path
 inline uint64_t apply_old_off() { return APPLY_DATA_OFF + 2 * SMALL_EDGES * sizeof(rg_edge); }
 
+// A node of the versioned label history (rg_history.cu).
+struct HistNode {
+  uint64_t begin;           // version the value holds from
+  unsigned long long pre;   // older node of the same vertex, ~0 if none
+  uint64_t value;
+};
+
 // A cached, instantiated level-loop graph.
 struct LoopGraph {
   cudaGraphExec_t exec = nullptr;
@@ -281,6 +288,10 @@ struct Graph {
   uint64_t sell_hubs = 0, sell_rows = 0, sell_slices = 0, sell_epoch = 0;
   uint64_t sell_cls[3] = {0, 0, 0};  // first slice of width <= 8, 4, 2
   uint64_t pull_div = 64;
+  // versioned label history (off until rg_history_enable)
+  HistNode *hist_nodes = nullptr;
+  unsigned long long *hist_head = nullptr, *hist_ctl = nullptr;  // ctl: pool top, error
+  uint64_t hist_cap = 0, hist_used = 0;
   uint64_t tiny_edges = 32768;  // frontiers with at most this many out-slots run in k_push_tiny (0: off)
   uint64_t adj_version = 1, pull_version = 0;
   int dense_pull = 2;  // dense build levels: 1 = pull over in-edges, 0 = edge-centric push, 2 = pull for WCC only
@@ -373,6 +384,12 @@ int tree_alloc(Graph &g);
 // conditional node, one graph launch and one synchronisation in all.
 int apply_small(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
                 uint64_t *old_num);
+// Versioned label history (rg_history.cu).
+int history_enable(Graph &g, uint64_t capacity);
+int history_record(Graph &g, uint64_t version, int all);
+int history_get(Graph &g, const uint64_t *vids, uint64_t n, uint64_t version, uint64_t *values, uint8_t *found);
+int history_gc(Graph &g, uint64_t version);
+void history_free(Graph &g);
 // An insert batch and a delete batch (each <= SMALL_EDGES) in one graph launch:
 // the two fused applies back to back, the delete one skipped if the insert
 // one stopped on a storage error.
