@@ -277,6 +277,11 @@ int rg_server_create(uint64_t hbm_budget_bytes, double target_epoch_ms, uint64_t
  * RG_ENOMEM_HBM when its device bytes would exceed the budget. */
 int rg_server_attach(rg_server *s, rg_graph *g, int algo, int directed, uint32_t *instance);
 int rg_server_detach(rg_server *s, uint32_t instance);
+/* Record the label history (rg_history_record of the modified vertices) after
+ * every epoch of the instance, at versions 1, 2, ...; the graph needs
+ * trace_modified and rg_history_enable.  version (nullable) receives the last
+ * version recorded so far. */
+int rg_server_history(rg_server *s, uint32_t instance, int enable, uint64_t *version);
 /* Thread-safe; timestamps the requests. */
 int rg_server_submit(rg_server *s, const rg_request *reqs, uint64_t n);
 /* Drain up to cap completions (n = number written). */

@@ -111,6 +111,7 @@ def _declare(L):
         "rg_server_create": [_u64, ctypes.c_double, _u64, _int, P],
         "rg_server_attach": [P, P, _int, _int, P],
         "rg_server_detach": [P, ctypes.c_uint32],
+        "rg_server_history": [P, ctypes.c_uint32, _int, P],
         "rg_server_submit": [P, P, _u64],
         "rg_server_poll": [P, P, _u64, P],
         "rg_server_drain": [P, _u64],
@@ -487,6 +488,12 @@ class Server:
                "rg_server_attach")
         self._graphs[inst.value] = graph
         return inst.value
+
+    def history(self, instance: int, enable: bool = True) -> int:
+        """Record the label history after every epoch; returns the last version."""
+        v = np.zeros(1, np.uint64)
+        _check(lib().rg_server_history(self._h, int(instance), int(enable), _p(v)), "rg_server_history")
+        return int(v[0])
 
     def detach(self, instance: int):
         _check(lib().rg_server_detach(self._h, int(instance)), "rg_server_detach")

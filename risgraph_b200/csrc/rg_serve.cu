@@ -69,6 +69,8 @@ struct Instance {
   Sink *sink = nullptr;
   std::thread worker;
   uint64_t cap = 1;  // epoch cap, worker-owned
+  std::atomic<int> history{0};  // record the label history after every epoch
+  uint64_t version = 0;         // history version, worker-owned
   std::atomic<uint64_t> epochs{0}, applied{0};
 };
 
@@ -146,6 +148,9 @@ void worker_main(rg_server *s, Instance *in) {
       rc = rg_apply_add(in->g, in->algo, adds.data(), adds.size(), in->directed, nullptr);
     else if (!dels.empty())
       rc = rg_apply_del(in->g, in->algo, dels.data(), dels.size(), in->directed, nullptr);
+    // the modified vertices of the epoch go to the label history at the next
+    // version (src/sssp_inc_rt.cpp:338-343 records after every update)
+    if (!rc && in->history.load(std::memory_order_relaxed)) rc = rg_history_record(in->g, ++in->version, 0);
     const uint64_t t1 = now_ns();
     // Adapt the cap to keep one epoch within the target (cf. the threshold
     // update of src/sssp_inc_rt.cpp:394-412, driven by time instead of timeouts).
@@ -352,6 +357,22 @@ int rg_server_attach(rg_server *s, rg_graph *g, int algo, int directed, uint32_t
   Instance *raw = in.get();
   in->worker = std::thread([s, raw] { worker_main(s, raw); });
   *instance = in->id;
+  return RG_OK;
+}
+
+int rg_server_history(rg_server *s, uint32_t instance, int enable, uint64_t *version) {
+  if (!s) return RG_EINVAL;
+  std::shared_ptr<Instance> in = find(s, instance);
+  if (!in) {
+    rg::set_error("unknown instance");
+    return RG_EINVAL;
+  }
+  if (enable && !in->g->g.hist_nodes) {
+    rg::set_error("enable the graph's history (rg_history_enable) first");
+    return RG_ESTATE;
+  }
+  in->history.store(enable ? 1 : 0);
+  if (version) *version = in->version;  // the worker's latest recorded version
   return RG_OK;
 }
 

@@ -69,3 +69,33 @@ def test_history_needs_trace_and_reports_full_pool():
     assert e.value.status == 5  # RG_ENOSPACE
     assert g.history_nodes() == (100, 100)
     g.close()
+
+
+def test_served_epochs_record_history():
+    """A served instance with history on: after the load, version k holds the
+    values after k epochs, and the last version equals the current values."""
+    scale = 11
+    pairs = gen.rmat(scale, seed=43)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    g = rg.Graph(V, len(pairs), trace_modified=True, weighted=True)
+    g.add_pairs(pairs[:imported], True, want_old=False)
+    g.build_tree("sssp", 0)
+    g.history_enable(4 * V + 100000)
+    g.history_record(0, all_vertices=True)
+    before = g.values()
+    with rg.Server(max_epoch=256) as srv:
+        k = srv.attach(g)
+        srv.history(k, True)
+        srv.run_load([dict(instance=k, clients=8, pairs=pairs, imported=imported, max_updates=800,
+                           duration_s=30.0, think_us=20.0, weighted=True, seed=3)])
+        last = srv.history(k, True)
+        srv.detach(k)
+    assert last >= 1
+    vids = np.arange(V, dtype=np.uint64)
+    vals, found = g.history_get(vids, last)
+    assert found.all()
+    np.testing.assert_array_equal(vals, g.values())
+    vals0, _ = g.history_get(vids, 0)
+    np.testing.assert_array_equal(vals0, before)
+    g.close()
