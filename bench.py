@@ -66,6 +66,7 @@ def parse():
                     help="only the batched incremental sweep (SSSP and SSWP, batches 1..100k) on RMAT-<served-scale>")
     ap.add_argument("--served-mix", action="store_true",
                     help="only the six-instance served mix (RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default level-mode options")
     ap.add_argument("--wcc-deletions", action="store_true",
                     help="only incremental WCC with heavy deletion on an ER+RMAT mix of 2^wcc-scale vertices")
     ap.add_argument("--wcc-scale", type=int, default=26)
@@ -492,6 +493,8 @@ def main():
     g.add_pairs(pairs, directed, want_old=False)
     stream = torch.cuda.Stream()
     g.set_stream(stream.cuda_stream)
+    # the level-mode knobs for this graph, picked by the library's autotuner
+    tune = g.autotune(algo, root, reps=3) if not args.no_autotune else None
 
     for _ in range(max(args.warmup, 1)):
         g.build_tree(algo, root)
@@ -579,7 +582,7 @@ def main():
                 "config": workload(args), "clocks": clk.summary(),
                 "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": V * 8},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "reached": {"V_r": V_r, "E_r": E_r}, "served": served}
+                "reached": {"V_r": V_r, "E_r": E_r}, "autotune": tune, "served": served}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

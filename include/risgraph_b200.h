@@ -208,6 +208,23 @@ typedef enum {
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);
 
+/* Autotuner of the options above for this graph and algorithm: coordinate
+ * descent over candidate values of the pull / bottom-up divisor, the dense
+ * divisor, the edge-balanced minimum and the small-frontier size, timing `reps`
+ * full builds per trial (and, when n_sample > 0, insert + delete round trips
+ * of the sample batch, which leave the graph unchanged, for the small-frontier
+ * size).  The chosen values stay set on the graph.  Every trial must give the
+ * same values (checked by checksum); the labels end as after rg_build_tree.
+ * No reference counterpart: the reference's thresholds are constants. */
+typedef struct {
+  double build_ms_before, build_ms_after;  /* median build time */
+  double apply_ms_before, apply_ms_after;  /* median sample round trip (0 without a sample) */
+  uint64_t options[8];                     /* chosen values, indexed by rg_option */
+  uint64_t trials;
+} rg_tune_report;
+int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *sample, uint64_t n_sample, int directed,
+                int reps, rg_tune_report *out);
+
 /* Device bytes held by the graph. */
 int rg_device_bytes(rg_graph *g, uint64_t *bytes);
 

@@ -42,6 +42,12 @@ class ServerStats(ctypes.Structure):  # rg_server_stats
                 ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double)]
 
 
+class TuneReport(ctypes.Structure):  # rg_tune_report
+    _fields_ = [("build_ms_before", ctypes.c_double), ("build_ms_after", ctypes.c_double),
+                ("apply_ms_before", ctypes.c_double), ("apply_ms_after", ctypes.c_double),
+                ("options", ctypes.c_uint64 * 8), ("trials", ctypes.c_uint64)]
+
+
 class LoadConfig(ctypes.Structure):  # rg_load_config
     _fields_ = [("instance", ctypes.c_uint32), ("clients", ctypes.c_uint32), ("think_us", ctypes.c_double),
                 ("duration_s", ctypes.c_double), ("max_updates", ctypes.c_uint64), ("offset", ctypes.c_uint64),
@@ -103,6 +109,7 @@ def _declare(L):
         "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
         "rg_set_option": [P, _int, _u64],
         "rg_get_option": [P, _int, P],
+        "rg_autotune": [P, _int, _u64, P, _u64, _int, _int, P],
         "rg_history_enable": [P, _u64],
         "rg_history_record": [P, _u64, _int],
         "rg_history_get": [P, P, _u64, _u64, P, P],
@@ -342,6 +349,19 @@ class Graph:
 
     def values(self) -> np.ndarray:
         return self.labels(True, False, False)[0]
+
+    def autotune(self, algo: str, root: int = 0, sample=None, directed: bool = True, reps: int = 5) -> dict:
+        """rg_autotune: pick the level-mode options for this graph; returns the report."""
+        rep = TuneReport()
+        e = as_edges(sample) if sample is not None else None
+        _check(lib().rg_autotune(self._h, ALGOS[algo], int(root), _p(e), 0 if e is None else len(e), int(directed),
+                                 int(reps), ctypes.byref(rep)), "rg_autotune")
+        self.algo = algo
+        names = {v: k for k, v in self.OPTIONS.items()}
+        return {"build_ms_before": rep.build_ms_before, "build_ms_after": rep.build_ms_after,
+                "apply_ms_before": rep.apply_ms_before, "apply_ms_after": rep.apply_ms_after,
+                "options": {names[i]: int(rep.options[i]) for i in range(8) if i in names},
+                "trials": int(rep.trials)}
 
     # -- versioned label history (MVVec, core/mvvec.hpp)
     def history_enable(self, capacity_nodes: int):

@@ -31,7 +31,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompiler", "-fPIC",
                   "-I" + INCLUDE, "-I" + CSRC, "--expt-relaxed-constexpr"]
 
-CU_SOURCES = ["rg_api.cu", "rg_storage.cu", "rg_tree.cu", "rg_static.cu", "rg_serve.cu", "rg_history.cu"]
+CU_SOURCES = ["rg_api.cu", "rg_storage.cu", "rg_tree.cu", "rg_static.cu", "rg_serve.cu", "rg_history.cu", "rg_autotune.cu"]
 C_SOURCES = ["rg_gen.c"]
 HEADERS = ["rg_internal.cuh", "rg_storage_dev.cuh"]
 

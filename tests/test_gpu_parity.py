@@ -410,3 +410,24 @@ def test_apply_add_del_one_submission(algo, batch):
         g.apply_add_del(algo, adds, dels, directed)
         assert g.checksum() == int(ref[k]), f"batch {k}"
     check_tree(g, og)
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp"])
+def test_autotune_keeps_values(algo):
+    """rg_autotune only picks kernels: the tuned graph's values equal the
+    oracle's, and the chosen options are among the candidates."""
+    scale = 14
+    pairs = gen.rmat(scale, seed=12)
+    V = 1 << scale
+    root = gen.max_out_degree_vertex(pairs, V)
+    imported = int(len(pairs) * 0.95)
+    g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs))
+    og = oracle_graph(algo, V, pairs[:imported])
+    sample = edges_of(algo, pairs[imported:imported + 64])
+    rep = g.autotune(algo, root, sample=sample, reps=3)
+    assert rep["trials"] >= 10
+    assert rep["build_ms_after"] > 0 and rep["apply_ms_after"] > 0
+    assert rep["options"]["tiny_edges"] in (0, 8192, 32768, 131072)
+    og.build_tree(root)
+    np.testing.assert_array_equal(g.values(), og.labels()[0])
+    check_tree(g, og, root)
