@@ -41,6 +41,40 @@ def test_build_tree_parity(algo, scale):
     np.testing.assert_array_equal(g.values(), val)
 
 
+PUSH_MODES = {
+    # every level of the build in one push mode
+    "edge_balanced": {"lbs_min": 1, "dense_div": 1},
+    "dense": {"dense_div": 1 << 30},
+    "sparse": {"lbs_min": 1 << 40, "dense_div": 1},
+}
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("mode", sorted(PUSH_MODES))
+def test_build_tree_parity_push_modes(algo, mode):
+    """Builds pushed level by level in one mode: the edge-balanced and dense
+    modes commit each level through per-vertex packed keys, the sparse mode
+    through the 16-byte CAS; values equal the oracle's, trees are valid, and
+    an incremental batch on top still matches."""
+    scale = 13
+    V = 1 << scale
+    pairs = gen.er_rmat_mix(scale, 24 * V, seed=17)
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = gpu_graph(algo, V, pairs)
+    for k, v in {"dense_pull": 0, "bfs_bottom_up": 0, "tiny_edges": 0, **PUSH_MODES[mode]}.items():
+        g.set_option(k, v)
+    og = oracle_graph(algo, V, pairs)
+    og.build_tree(root)
+    g.build_tree(algo, root)
+    val = check_tree(g, og, root)
+    np.testing.assert_array_equal(val, og.labels()[0])
+    extra = gen.rmat(scale, 2000, seed=23)
+    g.apply_add_pairs(algo, extra, directed=(algo != "wcc"))
+    og2 = oracle_graph(algo, V, np.concatenate([pairs, extra]))
+    og2.build_tree(root)
+    np.testing.assert_array_equal(check_tree(g, og2, root), og2.labels()[0])
+
+
 @pytest.mark.parametrize("algo", ALGOS)
 def test_build_tree_parity_er_rmat_mix(algo):
     """Half uniform, half RMAT endpoints: nearly every vertex has in-edges and
