@@ -41,6 +41,43 @@ def test_build_tree_parity(algo, scale):
     np.testing.assert_array_equal(g.values(), val)
 
 
+@pytest.mark.parametrize("algo", ALGOS)
+def test_build_tree_parity_pull_levels(algo):
+    """Every large level pulls over the sliced in-edge copy, BFS included (no
+    bottom-up levels)."""
+    scale = 14
+    V = 1 << scale
+    pairs = gen.er_rmat_mix(scale, 32 * V, seed=29)
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = gpu_graph(algo, V, pairs)
+    g.set_option("dense_pull", 1)
+    g.set_option("bfs_bottom_up", 0)
+    og = oracle_graph(algo, V, pairs)
+    og.build_tree(root)
+    g.build_tree(algo, root)
+    np.testing.assert_array_equal(check_tree(g, og, root), og.labels()[0])
+
+
+def test_build_tree_parity_values_beyond_16_bits():
+    """Large SSSP distances through pull levels: a 700-hop chain from the root
+    ends in a vertex with 4,000 out-edges into a random graph, so the large
+    frontiers that pull hold values past 65,535."""
+    V = 1 << 14
+    rng = np.random.default_rng(31)
+    chain = np.stack([np.arange(0, 699), np.arange(1, 700)], axis=1)
+    fan = np.stack([np.full(4000, 699), rng.integers(700, V, 4000)], axis=1)
+    rest = rng.integers(700, V, size=(16 * V, 2))
+    pairs = np.concatenate([chain, fan, rest]).astype(np.uint64)
+    g = gpu_graph("sssp", V, pairs)
+    og = oracle_graph("sssp", V, pairs)
+    og.build_tree(0)
+    g.build_tree("sssp", 0)
+    val = check_tree(g, og, 0)
+    np.testing.assert_array_equal(val, og.labels()[0])
+    reached = val[val < (1 << 27)]
+    assert reached.max() > 65535 and np.median(reached) > 65535
+
+
 PUSH_MODES = {
     # every level of the build in one push mode
     "edge_balanced": {"lbs_min": 1, "dense_div": 1},
