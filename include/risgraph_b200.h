@@ -194,7 +194,10 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
  *   RG_OPT_BFS_BU_DIV     a BFS build level goes bottom-up when frontier * div >= |V|
  *                         (default 64; Beamer's direction switch by frontier size)
  *   RG_OPT_RECOMPUTE_MIN  deletion repair falls back to a full build when the
- *                         invalidated set exceeds max(this, |V|/20) */
+ *                         invalidated set exceeds max(this, |V|/20)
+ *   RG_OPT_PULL_SPLIT     pull levels run the longest in-lists in a first launch
+ *                         so the rest read this level's hub values: 1 always,
+ *                         0 never, 2 (default) for SSSP and WCC */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -203,7 +206,8 @@ typedef enum {
   RG_OPT_RECOMPUTE_MIN = 4,
   RG_OPT_BFS_BU_DIV = 5,
   RG_OPT_PULL_DIV = 6,
-  RG_OPT_TINY_EDGES = 7
+  RG_OPT_TINY_EDGES = 7,
+  RG_OPT_PULL_SPLIT = 8
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);
@@ -219,7 +223,7 @@ int rg_get_option(rg_graph *g, int option, uint64_t *value);
 typedef struct {
   double build_ms_before, build_ms_after;  /* median build time */
   double apply_ms_before, apply_ms_after;  /* median sample round trip (0 without a sample) */
-  uint64_t options[8];                     /* chosen values, indexed by rg_option */
+  uint64_t options[16];                    /* chosen values, indexed by rg_option */
   uint64_t trials;
 } rg_tune_report;
 int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *sample, uint64_t n_sample, int directed,

@@ -45,7 +45,7 @@ class ServerStats(ctypes.Structure):  # rg_server_stats
 class TuneReport(ctypes.Structure):  # rg_tune_report
     _fields_ = [("build_ms_before", ctypes.c_double), ("build_ms_after", ctypes.c_double),
                 ("apply_ms_before", ctypes.c_double), ("apply_ms_after", ctypes.c_double),
-                ("options", ctypes.c_uint64 * 8), ("trials", ctypes.c_uint64)]
+                ("options", ctypes.c_uint64 * 16), ("trials", ctypes.c_uint64)]
 
 
 class LoadConfig(ctypes.Structure):  # rg_load_config
@@ -360,7 +360,7 @@ class Graph:
         names = {v: k for k, v in self.OPTIONS.items()}
         return {"build_ms_before": rep.build_ms_before, "build_ms_after": rep.build_ms_after,
                 "apply_ms_before": rep.apply_ms_before, "apply_ms_after": rep.apply_ms_after,
-                "options": {names[i]: int(rep.options[i]) for i in range(8) if i in names},
+                "options": {names[i]: int(rep.options[i]) for i in range(16) if i in names},
                 "trials": int(rep.trials)}
 
     # -- versioned label history (MVVec, core/mvvec.hpp)
@@ -434,7 +434,7 @@ class Graph:
         return sizes, int(e[0])
 
     OPTIONS = {"dense_pull": 0, "dense_div": 1, "lbs_min": 2, "bfs_bottom_up": 3, "recompute_min": 4, "bu_div": 5,
-               "pull_div": 6, "tiny_edges": 7}
+               "pull_div": 6, "tiny_edges": 7, "pull_split": 8}
 
     def set_option(self, name: str, value: int):
         _check(lib().rg_set_option(self._h, self.OPTIONS[name], int(value)), "rg_set_option")

@@ -511,6 +511,10 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
     case RG_OPT_BFS_BU_DIV: g.bu_div = value ? value : 1; return RG_OK;
     case RG_OPT_PULL_DIV: g.pull_div = value ? value : 1; return RG_OK;
     case RG_OPT_TINY_EDGES: g.tiny_edges = value; return RG_OK;
+    case RG_OPT_PULL_SPLIT:
+      if (value > 2) break;
+      g.pull_split = (int)value;
+      return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -528,6 +532,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_BFS_BU_DIV: *value = g.bu_div; return RG_OK;
     case RG_OPT_PULL_DIV: *value = g.pull_div; return RG_OK;
     case RG_OPT_TINY_EDGES: *value = g.tiny_edges; return RG_OK;
+    case RG_OPT_PULL_SPLIT: *value = (uint64_t)g.pull_split; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

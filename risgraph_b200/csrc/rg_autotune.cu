@@ -126,8 +126,9 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
   *out = rg_tune_report{};
   if ((rc = t.build_ms(&out->build_ms_before))) return rc;
   if ((rc = t.apply_ms(&out->apply_ms_before))) return rc;
-  uint64_t orig[8];
-  for (int o = 0; o < 8; o++) rg_get_option(g, o, &orig[o]);
+  constexpr int NOPT = RG_OPT_PULL_SPLIT + 1;
+  uint64_t orig[NOPT];
+  for (int o = 0; o < NOPT; o++) rg_get_option(g, o, &orig[o]);
   double ms = 0;
   // build knobs
   if (algo == RG_BFS) {
@@ -135,6 +136,7 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
   } else {
     if ((rc = t.tune(RG_OPT_PULL_DIV, {16, 32, 64, 128, 256}, &Tuner::build_ms, &ms))) return rc;
   }
+  if (algo != RG_BFS && (rc = t.tune(RG_OPT_PULL_SPLIT, {0, 1}, &Tuner::build_ms, &ms))) return rc;
   if ((rc = t.tune(RG_OPT_DENSE_DIV, {10, 20, 40, 80}, &Tuner::build_ms, &ms))) return rc;
   if ((rc = t.tune(RG_OPT_LBS_MIN, {512, 2048, 8192, 32768}, &Tuner::build_ms, &ms))) return rc;
   // small-frontier knob: builds and the sample's round trips together
@@ -143,11 +145,11 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
   if ((rc = t.apply_ms(&out->apply_ms_after))) return rc;
   if (out->build_ms_after + out->apply_ms_after > 1.05 * (out->build_ms_before + out->apply_ms_before)) {
     // the knobs interact; when their combination lost, keep the settings the graph had
-    for (int o = 0; o < 8; o++) rg_set_option(g, o, orig[o]);
+    for (int o = 0; o < NOPT; o++) rg_set_option(g, o, orig[o]);
     if ((rc = t.build_ms(&out->build_ms_after))) return rc;
     if ((rc = t.apply_ms(&out->apply_ms_after))) return rc;
   }
-  for (int o = 0; o < 8; o++) rg_get_option(g, o, &out->options[o]);
+  for (int o = 0; o < NOPT; o++) rg_get_option(g, o, &out->options[o]);
   out->trials = t.trials;
   // leave the labels of a fresh build, as rg_build_tree would
   return rg_build_tree(g, algo, root, nullptr);

@@ -287,7 +287,9 @@ struct Graph {
   unsigned long long *sell_cnt = nullptr;
   uint64_t sell_hubs = 0, sell_rows = 0, sell_slices = 0, sell_epoch = 0;
   uint64_t sell_cls[3] = {0, 0, 0};  // first slice of width <= 8, 4, 2
+  uint64_t sell_split = 0;           // first slice of the second launch of a pull level
   uint64_t pull_div = 64;
+  int pull_split = 2;  // two-launch pull levels: 1 always, 0 never, 2 SSSP and WCC
   // versioned label history (off until rg_history_enable)
   HistNode *hist_nodes = nullptr;
   unsigned long long *hist_head = nullptr, *hist_ctl = nullptr;  // ctl: pool top, error

@@ -575,8 +575,25 @@ __global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint
 // no atomics on labels: a vertex row is written only by its own lane; a piece
 // leaves its best in a side array and k_pull_hub_fix combines the pieces of
 // each hub.
-constexpr uint32_t PULL_HUB = 1024;
+constexpr uint32_t PULL_HUB = 512;
 constexpr int PS_TPB = 256;
+// Split pull levels (RG_OPT_PULL_SPLIT): a level runs in two launches, first
+// the slices of the longest in-lists (width >= PULL_SPLIT: the hubs and their
+// pieces), then k_pull_hub_fix, then every other slice.  The second launch
+// reads the hubs' values of this level (a value cached in L1 by the first
+// launch is not carried into the second), where one launch reads them stale
+// from L1 for most of the level, so values move along hub paths faster and
+// fewer levels pull.  On RMAT-22 the WCC build pulls 2 levels instead of 3
+// (1.15 ms against 1.47 unsplit), SSSP 4 instead of 5 (3.96 x E entries read
+// against 4.88; 1.70 ms against 1.73).  The first launch has few, long slices
+// and leaves part of the GPU idle at its end; SSWP, whose values settle in
+// fewer levels anyway, loses more there than it saves (2.00 ms against 1.89),
+// so by default SSSP and WCC split and SSWP does not.
+// Without the split the level is one launch over every slice, k_pull_hub_fix,
+// and an empty launch (every level runs the same three kernels).
+constexpr uint32_t PULL_SPLIT = 256;
+// every hub piece (at least PULL_HUB / 2 entries) must fall in the first launch
+static_assert(PULL_SPLIT <= PULL_HUB / 2, "hub pieces must be pulled before k_pull_hub_fix");
 // In-list entries a lane keeps in flight: 16 for 8-byte weighted entries; 8 for
 // 4-byte ones, plus the next 8 prefetched (measured best on RMAT-22).
 template <bool W>
@@ -802,10 +819,13 @@ __device__ __forceinline__ void pull_narrow(const DevGraph &g, const typename Se
   }
 }
 
+// One launch covers the wide slices [s_lo, s_hi), and the narrow classes
+// when `rest` is set.
 template <int A, bool W>
 __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename SellE<W>::E *ent, const uint64_t *off,
                                                       const uint32_t *row_id, uint64_t rows, uint64_t slices,
-                                                      PullClasses cls, ulonglong2 *piece_best, uint32_t *fout,
+                                                      PullClasses cls, uint64_t s_lo, uint64_t s_hi, int rest,
+                                                      ulonglong2 *piece_best, uint32_t *fout,
                                                       unsigned long long *fout_n, uint32_t mst) {
   if (g.ctl[C_MODE] != M_PULL) return;
   using S_ = SellE<W>;
@@ -813,7 +833,7 @@ __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long local = 0;
-  for (uint64_t s = warp; s < cls.c8; s += nwarps) {
+  for (uint64_t s = s_lo + warp; s < s_hi; s += nwarps) {
     const uint64_t r = s * 32 + lane;
     const bool active = r < rows;
     const uint32_t id = active ? row_id[r] : 0u;
@@ -847,6 +867,10 @@ __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename
     }
     pull_row_done<A>(g, active, id, has, best, bsrc, bw, piece_best, fout, fout_n, mst, local);
   }
+  if (!rest) {
+    warp_add_result(local, &g.ctl[C_RESULT]);
+    return;
+  }
   pull_narrow<A, W, 2>(g, ent, off, row_id, rows, cls.c8, cls.c4, piece_best, fout, fout_n, mst, local, warp, nwarps);
   pull_narrow<A, W, 4>(g, ent, off, row_id, rows, cls.c4, cls.c2, piece_best, fout, fout_n, mst, local, warp, nwarps);
   pull_narrow<A, W, 8>(g, ent, off, row_id, rows, cls.c2, slices, piece_best, fout, fout_n, mst, local, warp, nwarps);
@@ -856,12 +880,14 @@ __global__ void __launch_bounds__(PS_TPB) k_pull_sell(DevGraph g, const typename
 
 // First slice whose width is at most 8, 4, 2 (slice widths never increase).
 __global__ void k_sell_classes(const uint32_t *sorted_key, uint64_t slices, unsigned long long *cls) {
+  // cls[3]: first slice narrower than PULL_SPLIT
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < slices; s += stride) {
     const uint32_t w = sorted_key[s * 32], wp = s ? sorted_key[(s - 1) * 32] : 0xFFFFFFFFu;
     if (w <= 8 && wp > 8) cls[0] = s;
     if (w <= 4 && wp > 4) cls[1] = s;
     if (w <= 2 && wp > 2) cls[2] = s;
+    if (w < PULL_SPLIT && wp >= PULL_SPLIT) cls[3] = s;
   }
 }
 
@@ -1077,7 +1103,7 @@ __global__ void k_prologue(DevGraph g, unsigned long long inv_tag) { prologue_ct
 __host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
   switch (mode) {
     case M_SPARSE: return 2;
-    case M_PULL: return 2;
+    case M_PULL: return 3;
     case M_DENSE_PUSH: return 2;
     case M_BOTTOM_UP: return 1;
     case M_LBS: return 5;
@@ -1091,6 +1117,7 @@ struct LevelCfg {
   uint64_t lbs_min;
   uint64_t bu_div;    // BFS builds go bottom-up once frontier * bu_div >= |V|
   uint64_t pull_div;  // builds pull once frontier * pull_div >= |V|
+  uint64_t pull_split;  // pull levels run in two launches
   uint64_t tiny_edges;
   int allow_pull;
   int bottom_up;
@@ -1827,12 +1854,12 @@ int prepare_pull_w(Graph &g) {
     e = cub::DeviceScan::ExclusiveSum(g.cub_tmp, tb, g.scratch64, g.sell_off, slices + 1, g.stream);
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(&total, g.sell_off + slices, 8, cudaMemcpyDeviceToHost, g.stream);
-  unsigned long long cls[3] = {slices, slices, slices};
-  if (e == cudaSuccess) e = cudaMemcpyAsync(g.sell_cnt + 2, cls, 24, cudaMemcpyHostToDevice, g.stream);
+  unsigned long long cls[4] = {slices, slices, slices, slices};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g.sell_cnt + 2, cls, 32, cudaMemcpyHostToDevice, g.stream);
   if (e == cudaSuccess) {
     count_launch(g);
     k_sell_classes<<<g.num_sms * 4, TPB, 0, g.stream>>>(key1, slices, g.sell_cnt + 2);
-    e = cudaMemcpyAsync(cls, g.sell_cnt + 2, 24, cudaMemcpyDeviceToHost, g.stream);
+    e = cudaMemcpyAsync(cls, g.sell_cnt + 2, 32, cudaMemcpyDeviceToHost, g.stream);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
   cudaFree(key0);
@@ -1850,6 +1877,7 @@ int prepare_pull_w(Graph &g) {
   g.sell_cls[2] = cls[2];
   g.sell_cls[1] = std::min<uint64_t>(cls[1], g.sell_cls[2]);
   g.sell_cls[0] = std::min<uint64_t>(cls[0], g.sell_cls[1]);
+  g.sell_split = std::min<uint64_t>(cls[3], g.sell_cls[0]);
   g.sell_epoch++;
   g.pull_version = g.adj_version;
   return RG_OK;
@@ -1858,6 +1886,11 @@ int prepare_pull_w(Graph &g) {
 // Dense build levels pull (sliced ELL) for SSSP / SSWP / WCC by default; BFS
 // builds use their bottom-up levels.  RG_OPT_DENSE_PULL 0 / 1 force push / pull.
 bool pull_on(const Graph &g, int A) { return g.dense_pull == 1 || (g.dense_pull == 2 && A != RG_BFS); }
+
+// Two-launch pull levels: RG_OPT_PULL_SPLIT 1 always, 0 never, 2 (default) for SSSP and WCC.
+bool pull_split_on(const Graph &g, int A) {
+  return g.pull_split == 1 || (g.pull_split == 2 && (A == RG_SSSP || A == RG_WCC));
+}
 
 int prepare_pull(Graph &g) {
   if (g.pull_version == g.adj_version) return RG_OK;
@@ -1880,14 +1913,21 @@ int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
       k_push<A, W><<<g.num_sms * 16, TPB, 0, s>>>(g.d, fin, fin_n, fout, fout_n, g.hubq, hub_n, mst);
       k_push_hub<A, W><<<g.num_sms * 8, TPB, 0, s>>>(g.d, g.hubq, hub_n, fout, fout_n, mst);
       break;
-    case M_PULL:
-      k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(
-          g.d, reinterpret_cast<const typename SellE<W>::E *>(g.sell_ent), g.sell_off, g.sell_row, g.sell_rows,
-          g.sell_slices, PullClasses{g.sell_cls[0], g.sell_cls[1], g.sell_cls[2]}, g.sell_piece_best, fout, fout_n,
-          mst);
+    case M_PULL: {
+      const auto *ent = reinterpret_cast<const typename SellE<W>::E *>(g.sell_ent);
+      const PullClasses cls{g.sell_cls[0], g.sell_cls[1], g.sell_cls[2]};
+      const bool split = pull_split_on(g, A);
+      const uint64_t mid = split ? g.sell_split : cls.c8;  // end of the first launch's wide slices
+      k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(g.d, ent, g.sell_off, g.sell_row, g.sell_rows, g.sell_slices,
+                                                         cls, 0, mid, split ? 0 : 1, g.sell_piece_best, fout, fout_n,
+                                                         mst);
       k_pull_hub_fix<A><<<(unsigned)std::max<uint64_t>(1, (g.sell_hubs + 255) / 256), 256, 0, s>>>(
           g.d, g.sell_hub, g.sell_hub_off, g.sell_hubs, g.sell_piece_best, fout, fout_n, mst);
+      k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(g.d, ent, g.sell_off, g.sell_row, g.sell_rows, g.sell_slices,
+                                                         cls, mid, cls.c8, split ? 1 : 0, g.sell_piece_best, fout,
+                                                         fout_n, mst);
       break;
+    }
     case M_DENSE_PUSH:
       k_mark_active<<<g.num_sms * 8, TPB, 0, s>>>(g.d, fin, fin_n, g.act);
       k_push_dense<A, W><<<g.num_sms * 3, DN_TPB, 0, s>>>(g.d, g.act, fout, fout_n, mst);
@@ -1918,6 +1958,7 @@ uint64_t cfg_key(const LevelCfg &c) {
   h = splitmix64(h ^ c.lbs_min);
   h = splitmix64(h ^ c.bu_div);
   h = splitmix64(h ^ c.pull_div);
+  h = splitmix64(h ^ c.pull_split);
   h = splitmix64(h ^ c.tiny_edges);
   return splitmix64(h ^ ((uint64_t)c.allow_pull << 1) ^ (uint64_t)c.bottom_up);
 }
@@ -1930,6 +1971,7 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   cfg.bottom_up = (A == RG_BFS && build_variant && g.bfs_bottom_up) ? 1 : 0;
   cfg.bu_div = g.bu_div;
   cfg.pull_div = g.pull_div;
+  cfg.pull_split = pull_split_on(g, A) ? 1 : 0;
   cfg.tiny_edges = g.tiny_edges < TINY_EDGES ? g.tiny_edges : TINY_EDGES;
   return cfg;
 }

@@ -42,9 +42,10 @@ def test_build_tree_parity(algo, scale):
 
 
 @pytest.mark.parametrize("algo", ALGOS)
-def test_build_tree_parity_pull_levels(algo):
+@pytest.mark.parametrize("split", [0, 1])
+def test_build_tree_parity_pull_levels(algo, split):
     """Every large level pulls over the sliced in-edge copy, BFS included (no
-    bottom-up levels)."""
+    bottom-up levels), in one launch or split (hub slices first)."""
     scale = 14
     V = 1 << scale
     pairs = gen.er_rmat_mix(scale, 32 * V, seed=29)
@@ -52,6 +53,7 @@ def test_build_tree_parity_pull_levels(algo):
     g = gpu_graph(algo, V, pairs)
     g.set_option("dense_pull", 1)
     g.set_option("bfs_bottom_up", 0)
+    g.set_option("pull_split", split)
     og = oracle_graph(algo, V, pairs)
     og.build_tree(root)
     g.build_tree(algo, root)
