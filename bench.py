@@ -538,7 +538,7 @@ def main():
     assert np.array_equal(host_vals, values)
     e2e = replica_throughput(E_r * args.steps, world, e2e_s)
 
-    # roofline of the level-relaxation kernels (k_push + k_push_hub)
+    # roofline of the level kernels of one build (every level's mode kernels, timed per level)
     g.profile(True)
     g.profile_read()
     nb = 3
@@ -554,8 +554,16 @@ def main():
     alg = algorithmic_bytes(V, V_r, E_r, algo)
     peak, peak_kind = load_peaks()
     achieved = alg / (push_ms_per_build / 1e3) / 1e9
+    traffic, traffic_src = None, None
+    if algo == "sssp":
+        # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of every level kernel of one
+        # SSSP build, from an ncu capture of the RMAT-21 build (32,130,409 reached edges); the
+        # pull levels stream the in-edge copy, so the bytes grow with the reached edges
+        traffic = 1_497_410_816 * E_r / 32_130_409
+        traffic_src = "ncu capture of one RMAT-21 SSSP build, scaled by reached edges"
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": peak_kind, "traffic": None,
+            "peak_source": peak_kind, "traffic": traffic, "traffic_unit": "bytes per build",
+            "traffic_source": traffic_src,
             "kernel": "level kernels of one build (k_level_begin + the level mode's push/pull kernels, all levels)",
             "algorithmic_bytes": alg, "launches_per_build": plaunch / nb, "kernel_ms_per_build": push_ms_per_build}
 
