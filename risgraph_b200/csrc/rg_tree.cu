@@ -2397,7 +2397,6 @@ int tree_alloc(Graph &g) {
   RG_CUDA(cudaMemset(g.d.modstamp, 0, V * 4 + 4));
   // labels start as "no parent", value 0 until build_tree (alloc_vertex_tree_array, :255-262)
   RG_CUDA(cudaMemset(g.d.lab, 0, V * 16 + 16));
-  for (uint64_t v = 0; v < 1; v++) {}
   return RG_OK;
 }
 
