@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(DN_TPB, 3) k_push_dense(DevGraph g, const uint
 // no atomics on labels: a vertex row is written only by its own lane; a piece
 // leaves its best in a side array and k_pull_hub_fix combines the pieces of
 // each hub.
-constexpr uint32_t PULL_HUB = 512;
+constexpr uint32_t PULL_HUB = 576;
 constexpr int PS_TPB = 256;
 // Split pull levels (RG_OPT_PULL_SPLIT): a level runs in two launches, first
 // the slices of the longest in-lists (width >= PULL_SPLIT: the hubs and their
@@ -588,10 +588,13 @@ constexpr int PS_TPB = 256;
 // against 4.88; 1.70 ms against 1.73).  The first launch has few, long slices
 // and leaves part of the GPU idle at its end; SSWP, whose values settle in
 // fewer levels anyway, loses more there than it saves (2.00 ms against 1.89),
-// so by default SSSP and WCC split and SSWP does not.
+// so by default SSSP and WCC split and SSWP does not.  Pieces of at most 576
+// entries and a split at width 288 keep the first launch within one wave of
+// resident warps (2,168 slices for 2,368 warps on RMAT-22; with 512 / 256 it
+// was 2,590 slices, and its last warp ran 42 iterations instead of 36).
 // Without the split the level is one launch over every slice, k_pull_hub_fix,
 // and an empty launch (every level runs the same three kernels).
-constexpr uint32_t PULL_SPLIT = 256;
+constexpr uint32_t PULL_SPLIT = 288;
 // every hub piece (at least PULL_HUB / 2 entries) must fall in the first launch
 static_assert(PULL_SPLIT <= PULL_HUB / 2, "hub pieces must be pulled before k_pull_hub_fix");
 // In-list entries a lane keeps in flight: 16 for 8-byte weighted entries; 8 for
