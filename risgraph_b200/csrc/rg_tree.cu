@@ -587,7 +587,7 @@ constexpr int PS_TPB = 256;
 // (1.15 ms against 1.47 unsplit), SSSP 4 instead of 5 (3.96 x E entries read
 // against 4.88; 1.70 ms against 1.73).  The first launch has few, long slices
 // and leaves part of the GPU idle at its end; SSWP, whose values settle in
-// fewer levels anyway, loses more there than it saves (2.00 ms against 1.89),
+// fewer levels anyway, loses more there than it saves (2.05 ms against 1.89),
 // so by default SSSP and WCC split and SSWP does not.  Pieces of at most 576
 // entries and a split at width 288 keep the first launch within one wave of
 // resident warps (2,168 slices for 2,368 warps on RMAT-22; with 512 / 256 it
