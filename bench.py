@@ -1,26 +1,34 @@
 #!/usr/bin/env python
-"""Full-graph dependency-tree build on RMAT-22: GTEPS through the C ABI.
+"""Dependency-tree maintenance on one B200: the headline full-graph build plus
+every benchmark configuration, each checked against the reference.
 
-Workload (one step): build_tree from scratch (core/graph.hpp:873-985) of
-SSSP (default; --algo bfs|sssp|sswp|wcc) over a directed RMAT graph of scale 22
-(4,194,304 vertices, 67,108,864 edges, a/b/c = .57/.19/.19, duplicates and
-self-loops kept, seeded order), weights splitmix64(src<<32|dst) % 255 + 1,
-rooted at the highest out-degree vertex.  The graph is resident in HBM; the
-edge pool (>0.5 GB) is larger than L2, so no flush is needed between steps.
+Headline (`value`): build_tree from scratch (core/graph.hpp:873-985) of SSSP
+(--algo) over a directed RMAT graph of scale 22 (4,194,304 vertices,
+67,108,864 edges, a/b/c = .57/.19/.19, duplicates and self-loops kept, seeded
+order), weights splitmix64(src<<32|dst) % 255 + 1, rooted at the highest
+out-degree vertex.  The graph is resident in HBM; the edge pool (>0.5 GB) is
+larger than L2, so no flush is needed between steps.
 
 value  = reached edges / device time per build (GTEPS), CUDA events on the
          stream the library launches on, max over ranks.
 e2e    = the same through the public API with the result read back: every
          step calls rg_build_tree and copies the value array into pinned host
          memory; wall clock.
-served = (N=1) the served incremental path: closed-loop clients stream sliding-
-         window inserts and deletes of an RMAT-24 SSSP instance through the
-         rg_server API (host buffers in, completions out); best updates/s at
-         p99 <= 1 ms for the batched server and for the plain one-update-per-
-         launch path, and their ratio.
---impl reference runs the reference's own CPU build_tree (oracle/_ref, the
-reference's core/graph.hpp compiled with an OpenMP stand-in for TBB) on the
-host cores.  Multi-GPU: independent replicas, one per rank (the path does not
+roofline = algorithmic bytes of one build / the device time per build of the
+         timed region, against the measured copy bandwidth.
+
+Extra legs of the default run (N=1, rank 0), each with a parity flag from the
+reference's own code (oracle/_ref/ref_driver: the reference's core/graph.hpp
+compiled unmodified) and the reference timed on all host cores:
+  builds      the other three algorithms of the RMAT-22 configuration
+  bfs_inc     plain incremental BFS, RMAT-16, 10,000 sliding-window steps
+  batches     batched incremental SSSP and SSWP, RMAT-24, batches 1..100,000
+  served      served incremental SSSP, RMAT-24, closed-loop clients
+  served_mix  six resident instances (RMAT 16..24), open-loop Poisson clients
+  wcc_del     incremental WCC with heavy deletion (ER+RMAT mix)
+--legs picks a subset.  --impl reference runs the reference's own CPU
+build_tree on the host cores (it generates its own input; this package is not
+loaded).  Multi-GPU: independent replicas, one per rank (the path does not
 shard); no collective on the data path.
 """
 from __future__ import annotations
@@ -41,11 +49,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "updates/s at p99≤1ms (served vs per-update GPU); full-graph GTEPS vs HBM"
 WEIGHTED = {"bfs": False, "sssp": True, "sswp": True, "wcc": False}
+UNREACHED = {"bfs": 65536, "sssp": 134217728, "sswp": 0}
 THROTTLE_BITS = {
     0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
     0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
     0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
 }
+ALL_LEGS = ["builds", "bfs_inc", "batches", "served", "served_mix", "wcc_del"]
 
 
 def parse():
@@ -57,20 +67,23 @@ def parse():
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--algo", default="sssp", choices=list(WEIGHTED))
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-timeout", type=float, default=240.0)
-    ap.add_argument("--served-scale", type=int, default=24, help="RMAT scale of the served instance (0 = skip)")
+    ap.add_argument("--legs", default=",".join(ALL_LEGS),
+                    help="comma-separated extra legs (" + ",".join(ALL_LEGS) + "), or 'none'")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip every reference run")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default level-mode options")
+    ap.add_argument("--served-scale", type=int, default=24, help="RMAT scale of the served and batched legs")
     ap.add_argument("--served-seconds", type=float, default=1.0, help="load duration per client count")
     ap.add_argument("--think-us", type=float, default=50.0, help="mean exponential think time per client")
-    ap.add_argument("--batch-sweep", action="store_true",
-                    help="only the batched incremental sweep (SSSP and SSWP, batches 1..100k) on RMAT-<served-scale>")
-    ap.add_argument("--served-mix", action="store_true",
-                    help="only the six-instance served mix (RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC)")
-    ap.add_argument("--no-autotune", action="store_true", help="keep the default level-mode options")
-    ap.add_argument("--wcc-deletions", action="store_true",
-                    help="only incremental WCC with heavy deletion on an ER+RMAT mix of 2^wcc-scale vertices")
-    ap.add_argument("--wcc-scale", type=int, default=26)
+    ap.add_argument("--mix-think-us", type=float, default=1000.0,
+                    help="mean interval between one open-loop client's updates in served_mix")
+    ap.add_argument("--wcc-scale", type=int, default=22, help="vertices 2^s of the heavy-deletion WCC leg")
     ap.add_argument("--wcc-updates", type=int, default=1000000)
+    ap.add_argument("--wcc-ref-max-scale", type=int, default=26,
+                    help="largest wcc_del scale whose result is replayed through the reference")
+    ap.add_argument("--wcc-deletions", action="store_true", help="only the heavy-deletion WCC leg")
+    ap.add_argument("--batch-sweep", action="store_true", help="only the batched incremental leg")
+    ap.add_argument("--served-mix", action="store_true", help="only the six-instance served mix")
+    ap.add_argument("--ref-timeout", type=float, default=900.0)
     return ap.parse_args()
 
 
@@ -82,14 +95,6 @@ def workload(args):
             "l2": "inputs larger than L2 (edge pool > 126 MB); no flush"}
 
 
-def make_graph_input(args):
-    from risgraph_b200 import gen
-    pairs = gen.rmat(args.scale, seed=args.seed)
-    V = 1 << args.scale
-    root = gen.max_out_degree_vertex(pairs, V)
-    return pairs, V, root
-
-
 def reached_edges(pairs, V, values, algo):
     """Distinct stored edges out of reached vertices (both directions for WCC)."""
     src = pairs[:, 0].astype(np.int64)
@@ -97,14 +102,15 @@ def reached_edges(pairs, V, values, algo):
     if algo == "wcc":
         key = np.unique(np.concatenate([src * V + dst, dst * V + src]))
         return int(len(key)), V
-    init = {"bfs": 65536, "sssp": 134217728, "sswp": 0}[algo]
-    reached = values != init
+    reached = values != UNREACHED[algo]
     key = np.unique(src * V + dst)
     ks = key // V
     return int(reached[ks].sum()), int(reached.sum())
 
 
 def algorithmic_bytes(V, V_r, E_r, algo):
+    """16 V (init value + parent) + 16 V_r (offset + own value of each reached
+    vertex) + E_r (S_e + 8), S_e = 16 weighted / 8 unweighted edge."""
     s_e = 16 if WEIGHTED[algo] else 8
     return 16 * V + 16 * V_r + E_r * (s_e + 8)
 
@@ -167,41 +173,41 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_reference(pairs, V, root, algo, repeats, warmup, timeout):
-    """The reference's own build_tree (oracle/_ref) on all host cores."""
+# ---------------------------------------------------------------- reference runs
+
+def ref_driver(mode, algo, graph, V, root, *args, timeout=900.0):
+    """The reference's own hot path (oracle/_ref/ref_driver) on all host cores,
+    threads pinned; returns ((info, arrays), None) or (None, reason)."""
     from oracle import oracle as O
     if not O.ref_available():
         return None, "oracle/_ref/ref_driver not built"
-    threads = os.cpu_count() or 1
-    with tempfile.TemporaryDirectory(prefix="rg_bench_") as tmp:
-        path = os.path.join(tmp, "g.bin")
-        pairs.tofile(path)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="true")
-        cmd = [O.REF_DRIVER, "build", algo, path, str(V), str(root), os.path.join(tmp, "out"), str(repeats),
-               str(warmup)]
-        try:
-            r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
-        except subprocess.TimeoutExpired:
-            return None, f"reference build timed out after {timeout}s"
-        if r.returncode != 0:
-            return None, f"reference driver failed: {r.stderr[-200:]}"
-        info = json.loads(r.stdout.strip().splitlines()[-1])
-        vals = np.fromfile(os.path.join(tmp, "out.val"), dtype=np.uint64)
-    info["threads"] = threads
-    return (info, vals), None
+    try:
+        return O.ref_run(mode, algo, graph, V, root, *args, timeout=timeout, bind=True), None
+    except subprocess.TimeoutExpired:
+        return None, f"reference {mode} timed out after {timeout:.0f}s"
+    except Exception as e:  # noqa: BLE001 - reported in the JSON line
+        return None, str(e)[-300:]
+
+
+def ref_cores():
+    return os.cpu_count() or 1
 
 
 def run_reference(args):
+    """--impl reference: the reference's own CPU build_tree on the host cores.
+    The driver generates the RMAT input itself (same generator, same seed) and
+    counts the reached edges over its own adjacency, so this process loads no
+    library of this package."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pairs, V, root = make_graph_input(args)
-    res, err = cpu_reference(pairs, V, root, args.algo, args.steps, args.warmup, 1800)
+    res, err = ref_driver("build", args.algo, f"rmat:{args.scale}:{args.seed}", 0, "maxdeg", args.steps, args.warmup,
+                          timeout=1800)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
-    info, vals = res
-    E_r, V_r = reached_edges(pairs, V, vals, args.algo)
+    info, _ = res
+    E_r = info["E_r"]
     t = float(np.mean(info["build_times"]))
     value = E_r / t / 1e9
     line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
@@ -210,26 +216,189 @@ def run_reference(args):
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": info["threads"], "kind": "reference",
                              "sample": f"RMAT-{args.scale} {args.algo} build_tree x{args.steps} after "
-                                       f"{args.warmup} warm-up (load {info['load_s']:.1f}s untimed)"},
+                                       f"{args.warmup} warm-up (generation and load {info['load_s']:.1f}s untimed)"},
             "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def served_leg(args):
-    """Served incremental SSSP: closed-loop clients with Poisson think times
-    send sliding-window inserts and deletes to a resident RMAT instance; the
-    client count doubles until p99 passes 1 ms.  Both the batched server and
-    the plain one-update-per-launch path run the same sweep; each reports its
-    best updates/s with p99 <= 1 ms.  After the sweeps, the incrementally
-    maintained distances must equal a from-scratch build of the final graph."""
+# ---------------------------------------------------------------- GPU legs
+
+def timed_builds(g, algo, root, steps, stream):
+    """Device ms of `steps` consecutive builds (CUDA events on the library's stream)."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for a, b in ev:
+        a.record(stream)
+        g.build_tree(algo, root)
+        b.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def leg_builds(args, peak):
+    """The other algorithms of the full-graph configuration: BFS, SSWP and WCC
+    (WCC undirected) builds on RMAT-22, each timed on the device and compared
+    with the reference's build of the same graph."""
+    import torch
+
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    scale = args.scale
+    pairs = gen.rmat(scale, seed=args.seed)
+    V = 1 << scale
+    root = gen.max_out_degree_vertex(pairs, V)
+    out = {}
+    for algo in ("bfs", "sswp", "wcc"):
+        directed = algo != "wcc"
+        g = rg.Graph(V, len(pairs), symmetric=not directed, weighted=WEIGHTED[algo])
+        g.add_pairs(pairs, directed, want_old=False)
+        stream = torch.cuda.Stream()
+        g.set_stream(stream.cuda_stream)
+        for _ in range(3):
+            g.build_tree(algo, root)
+        values = g.values()
+        ms = float(np.mean(timed_builds(g, algo, root, 20, stream)))
+        g.close()
+        E_r, V_r = reached_edges(pairs, V, values, algo)
+        alg = algorithmic_bytes(V, V_r, E_r, algo)
+        r = {"gteps": E_r / ms / 1e6, "ms_per_build": ms, "E_r": E_r, "V_r": V_r,
+             "roofline_frac": alg / (ms / 1e3) / 1e9 / peak}
+        if not args.no_cpu_baseline:
+            res, err = ref_driver("build", algo, f"rmat:{scale}:{args.seed}", V, root, 1, 0, timeout=args.ref_timeout)
+            if res is None:
+                r["reference"] = {"unavailable": err}
+            else:
+                info, arr = res
+                t = float(np.mean(info["build_times"]))
+                r["values_match_reference"] = bool(np.array_equal(arr["val"], values))
+                r["reference"] = {"gteps": info["E_r"] / t / 1e9, "cores": info["threads"], "E_r": info["E_r"]}
+        out[algo] = r
+    return out
+
+
+def leg_bfs_inc(args):
+    """Plain incremental BFS: RMAT-16, the first 90 % loaded, root 0, then
+    10,000 sliding-window steps (insert raw[i], delete raw[i - imported]), each
+    applied through the public API as one rg_apply_add_del; the value checksum
+    after every step is compared with the reference's (src/bfs_inc.cpp loop)."""
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    scale, steps = 16, 10000
+    pairs = gen.rmat(scale, seed=args.seed)
+    V = 1 << scale
+    E = len(pairs)
+    imported = int(E * 0.9)
+    g = rg.Graph(V, E, weighted=False)
+    g.add_pairs(pairs[:imported], True, want_old=False)
+    g.build_tree("bfs", 0)
+    edges = gen.edges_with_weights(pairs, False)
+    times = np.zeros(steps)
+    sums = np.zeros(steps, np.uint64)
+    for k in range(steps):
+        i = imported + k
+        t0 = time.perf_counter()
+        g.apply_add_del("bfs", edges[i:i + 1], edges[k:k + 1])
+        times[k] = time.perf_counter() - t0
+        sums[k] = g.checksum()
+    g.close()
+    out = {"workload": f"bfs_inc RMAT-{scale} (seed {args.seed}), 90% loaded, root 0, {steps} insert+delete steps",
+           "steps_per_s": steps / float(times.sum()), "p50_us": float(np.percentile(times, 50)) * 1e6,
+           "p99_us": float(np.percentile(times, 99)) * 1e6}
+    if not args.no_cpu_baseline:
+        res, err = ref_driver("inc", "bfs", f"rmat:{scale}:{args.seed}", V, 0, 0.9, steps, timeout=args.ref_timeout)
+        if res is None:
+            out["reference"] = {"unavailable": err}
+        else:
+            info, arr = res
+            rt = np.asarray(info["times"])
+            out["checksums_match_reference"] = bool(np.array_equal(arr["sums"][:steps], sums))
+            out["reference"] = {"steps_per_s": len(rt) / float(rt.sum()), "p50_us": float(np.percentile(rt, 50)) * 1e6,
+                                "p99_us": float(np.percentile(rt, 99)) * 1e6, "cores": info["threads"],
+                                "kind": "reference", "sample": f"the same {steps} steps"}
+    return out
+
+
+BATCH_PLAN = [(1, 100), (10, 100), (100, 50), (1000, 20), (10000, 5), (100000, 3)]
+
+
+def leg_batches(args):
+    """Batched incremental SSSP and SSWP on RMAT-24: the first 90 % loaded,
+    then consecutive sliding-window batches of 1, 10, 100, 1,000, 10,000 and
+    100,000 insert+delete pairs (src/sssp_inc_batch.cpp:136-181), each one
+    rg_apply_add_del through the public API (host buffers); the value checksum
+    after every batch is compared with the reference running the same batches."""
     import risgraph_b200 as rg
     from risgraph_b200 import gen
     scale = args.served_scale
     pairs = gen.rmat(scale, seed=args.seed)
     V = 1 << scale
-    imported = int(len(pairs) * 0.9)
+    E = len(pairs)
+    imported = int(E * 0.9)
     root = gen.max_out_degree_vertex(pairs, V)
-    g = rg.Graph(V, len(pairs), weighted=True)
+    spec = ",".join(f"{b}x{n}" for b, n in BATCH_PLAN)
+    out = {"workload": f"batched sliding window, RMAT-{scale} (seed {args.seed}), 90% loaded, root = max out-degree "
+                       f"vertex, batches (size x count) {spec}", "runs": {}}
+    for algo in ("sssp", "sswp"):
+        g = rg.Graph(V, E, weighted=True)
+        g.add_pairs(pairs[:imported], True, want_old=False)
+        g.build_tree(algo, root)
+        sums, per = [], []
+        lo = imported
+        for b, n in BATCH_PLAN:
+            ts = []
+            for _ in range(n):
+                adds = gen.edges_with_weights(pairs[lo:lo + b], True)
+                dels = gen.edges_with_weights(pairs[lo - imported:lo - imported + b], True)
+                t0 = time.perf_counter()
+                g.apply_add_del(algo, adds, dels)
+                ts.append(time.perf_counter() - t0)
+                sums.append(g.checksum())
+                lo += b
+            ts = np.asarray(ts)
+            per.append({"batch": b, "batches": n, "pairs_per_s": 2 * b * n / float(ts.sum()),
+                        "p50_ms": float(np.percentile(ts, 50)) * 1e3})
+        g.close()
+        r = {"gpu": per}
+        if not args.no_cpu_baseline:
+            res, err = ref_driver("sweep", algo, f"rmat:{scale}:{args.seed}", V, root, 0.9, spec,
+                                  timeout=args.ref_timeout)
+            if res is None:
+                r["reference"] = {"unavailable": err}
+            else:
+                info, arr = res
+                r["checksums_match_reference"] = bool(np.array_equal(arr["sums"], np.asarray(sums, np.uint64)))
+                rt = np.asarray(info["times"])
+                rp, k = [], 0
+                for b, n in BATCH_PLAN:
+                    seg = rt[k:k + n]
+                    k += n
+                    rp.append({"batch": b, "pairs_per_s": 2 * b * n / float(seg.sum()),
+                               "p50_ms": float(np.percentile(seg, 50)) * 1e3})
+                r["reference"] = {"runs": rp, "cores": info["threads"], "kind": "reference",
+                                  "sample": "the same batches"}
+        out["runs"][algo] = r
+    return out
+
+
+def leg_served(args):
+    """Served incremental SSSP: closed-loop clients with Poisson think times
+    send sliding-window inserts and deletes to a resident RMAT instance; the
+    client count doubles until p99 passes 1 ms.  Both the batched server and
+    the plain one-update-per-launch path run the same sweep; each reports its
+    best updates/s with p99 <= 1 ms.  After the sweeps, the incrementally
+    maintained distances must equal a from-scratch build of the final graph
+    and the reference's build of that graph.  The reference's own served
+    loop (the _inc_rt epoch loop) runs beside it on the host cores."""
+    import risgraph_b200 as rg
+    from risgraph_b200 import gen
+    scale = args.served_scale
+    pairs = gen.rmat(scale, seed=args.seed)
+    V = 1 << scale
+    E = len(pairs)
+    imported = int(E * 0.9)
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = rg.Graph(V, E, weighted=True)
     g.add_pairs(pairs[:imported], True, want_old=False)
     g.build_tree("sssp", root)
     offset = 0
@@ -267,79 +436,50 @@ def served_leg(args):
     b0, b1 = out["per_update"]["best_at_p99_le_1ms"], out["served"]["best_at_p99_le_1ms"]
     out["served_over_per_update"] = (b1["updates_per_s"] / b0["updates_per_s"]) if b0 and b1 else None
     g.close()
+    if not args.no_cpu_baseline:
+        # the final graph is the window [dels, imported + adds) of the stream
+        n_add, n_del = (offset + 1) // 2, offset // 2
+        res, err = ref_driver("build", "sssp", f"rmat:{scale}:{args.seed}@{n_del}:{imported + n_add}", V, root,
+                              timeout=args.ref_timeout)
+        if res is None:
+            out["values_match_reference"] = None
+            out["reference_build"] = {"unavailable": err}
+        else:
+            out["values_match_reference"] = bool(np.array_equal(res[1]["val"], inc))
+        clients = "64,256,1024"
+        res, err = ref_driver("rt", "sssp", f"rmat:{scale}:{args.seed}", V, root, 0.9, clients, 1, 1000000,
+                              timeout=args.ref_timeout)
+        if res is None:
+            out["reference"] = {"unavailable": err}
+        else:
+            info, _ = res
+            runs = info["runs"]
+            ok = [r for r in runs if r["p99_us"] <= 1000.0]
+            best = max(ok, key=lambda r: r["updates_per_s"]) if ok else None
+            out["reference"] = {"kind": "reference", "cores": info["threads"],
+                                "sample": f"the reference's _inc_rt epoch loop (src/sssp_inc_rt.cpp:119-441), "
+                                          f"closed-loop clients {clients}, 1,000,000 updates each, 1 ms timeout",
+                                "best_at_p99_le_1ms": best, "runs": runs}
     return out
 
 
-def max_over_ranks(x, dist):
-    """The slowest rank's time (every rank takes part; NCCL ranks reduce on
-    their GPU, gloo ranks on the CPU)."""
-    if not dist:
-        return float(x)
-    import torch
-    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
-    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+MIX = [(24, "sssp"), (23, "bfs"), (22, "wcc"), (20, "sssp"), (18, "bfs"), (16, "wcc")]
 
 
-def replica_throughput(units_per_rank, world, seconds):
-    """Whole-job GTEPS of `world` independent replicas, each processing
-    units_per_rank edges, timed by the slowest rank."""
-    return units_per_rank * world / seconds / 1e9
-
-
-def batch_sweep(args):
-    """Batched incremental SSSP / SSWP: the first 90% of an RMAT graph loaded,
-    then sliding-window batches of 1 .. 100,000 insert+delete pairs through
-    rg_apply_add_pairs / rg_apply_del_pairs (host buffers in); pairs/s and the
-    per-batch latency, then incremental == rebuild."""
-    import risgraph_b200 as rg
-    from risgraph_b200 import gen
-    scale = args.served_scale
-    pairs = gen.rmat(scale, seed=args.seed)
-    V = 1 << scale
-    E = len(pairs)
-    imported = int(E * 0.9)
-    root = gen.max_out_degree_vertex(pairs, V)
-    out = {"workload": f"batched incremental sliding window, RMAT-{scale}, first 90% loaded", "runs": []}
-    for algo in ("sssp", "sswp"):
-        g = rg.Graph(V, E, weighted=True)
-        g.add_pairs(pairs[:imported], True, want_old=False)
-        g.build_tree(algo, root)
-        lo = imported
-        for b in (1, 10, 100, 1000, 10000, 100000):
-            nb = int(min(4000, max(20, 3e6 // b)))
-            ts = []
-            for _ in range(nb):
-                if lo + b > E:
-                    break
-                t0 = time.perf_counter()
-                g.apply_add_pairs(algo, pairs[lo:lo + b])
-                g.apply_del_pairs(algo, pairs[lo - imported:lo - imported + b])
-                ts.append(time.perf_counter() - t0)
-                lo += b
-            ts = np.array(ts)
-            out["runs"].append({"algo": algo, "batch": b, "batches": len(ts),
-                                "pairs_per_s": 2 * b * len(ts) / float(ts.sum()),
-                                "p50_ms": float(np.percentile(ts, 50)) * 1e3,
-                                "p99_ms": float(np.percentile(ts, 99)) * 1e3})
-        inc = g.values()
-        g.build_tree(algo, root)
-        out[f"{algo}_incremental_equals_rebuild"] = bool(np.array_equal(inc, g.values()))
-        g.close()
-    return out
-
-
-def served_mix(args):
+def leg_served_mix(args):
     """Six resident instances of uneven size (RMAT 24 SSSP, 23 BFS, 22 WCC,
-    20 SSSP, 18 BFS, 16 WCC), admitted against an HBM budget, served together;
-    closed-loop clients (exponential think time) split evenly, doubled until
-    p99 passes 1 ms; the batched server against the per-update path."""
+    20 SSSP, 18 BFS, 16 WCC), admitted against an HBM budget, served together.
+    Open-loop Poisson clients (each issues an update at exponential intervals
+    of mean --mix-think-us, whether or not its earlier ones completed), split
+    evenly over the instances; the client count doubles from 64 until p99
+    passes 1 ms (the per-update path starts at 64 and halves while p99 is over
+    1 ms).  Per-instance p50/p99/p999 at every point.  Afterwards each
+    instance's values must equal a rebuild and, for scales <= 22, the
+    reference's build of the final graph."""
     import risgraph_b200 as rg
     from risgraph_b200 import gen
-    spec = [(24, "sssp"), (23, "bfs"), (22, "wcc"), (20, "sssp"), (18, "bfs"), (16, "wcc")]
     insts = []
-    for scale, algo in spec:
+    for scale, algo in MIX:
         pairs = gen.rmat(scale, seed=scale)
         V = 1 << scale
         imported = int(len(pairs) * 0.9)
@@ -349,55 +489,79 @@ def served_mix(args):
         g.build_tree(algo, root)
         insts.append(dict(scale=scale, algo=algo, pairs=pairs, imported=imported, g=g, root=root, offset=0))
     dev = sum(i["g"].device_bytes() for i in insts)
-    out = {"workload": "six instances RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC, sliding windows, "
-                       f"closed-loop clients, think {args.think_us:g} us", "device_bytes": dev}
+    out = {"workload": "six instances RMAT 24 SSSP, 23 BFS, 22 WCC, 20 SSSP, 18 BFS, 16 WCC (seed = scale), "
+                       "sliding windows, open-loop Poisson clients split evenly, mean interval "
+                       f"{args.mix_think_us:g} us per client, {args.served_seconds:g} s per point",
+           "device_bytes": dev}
+
+    def point(srv, ids, total):
+        per = max(1, total // len(insts))
+        loads = [dict(instance=k, clients=per, pairs=i["pairs"], imported=i["imported"],
+                      duration_s=args.served_seconds, think_us=args.mix_think_us, weighted=i["algo"] == "sssp",
+                      offset=i["offset"], seed=total, open_loop=1) for k, i in zip(ids, insts)]
+        res = srv.run_load(loads)
+        st = srv.stats(reset=True)
+        for i, r in zip(insts, res):
+            i["offset"] += r["adds"] + r["dels"]
+        return {"clients": per * len(insts), "updates_per_s": sum(r["updates_per_s"] for r in res),
+                "p50_us": st["p50_us"], "p99_us": st["p99_us"], "p999_us": st["p999_us"],
+                "per_instance": [{"scale": i["scale"], "algo": i["algo"], "updates_per_s": r["updates_per_s"],
+                                  "p50_us": r["p50_us"], "p99_us": r["p99_us"], "p999_us": r["p999_us"]}
+                                 for i, r in zip(insts, res)]}
+
     for mode, per_update in (("per_update", True), ("served", False)):
         sweep, best = [], None
         with rg.Server(hbm_budget_bytes=int(dev * 1.05), per_update=per_update, max_epoch=1 << 16,
                        target_epoch_ms=0.4) as srv:
             ids = [srv.attach(i["g"], directed=i["algo"] != "wcc") for i in insts]
-            per = 1
-            while per <= 1024:
-                loads = [dict(instance=k, clients=per, pairs=i["pairs"], imported=i["imported"],
-                              duration_s=args.served_seconds, think_us=args.think_us, weighted=i["algo"] == "sssp",
-                              offset=i["offset"], seed=per) for k, i in zip(ids, insts)]
-                res = srv.run_load(loads)
-                st = srv.stats(reset=True)
-                for i, r in zip(insts, res):
-                    i["offset"] += r["adds"] + r["dels"]
-                pt = {"clients": 6 * per, "updates_per_s": sum(r["updates_per_s"] for r in res),
-                      "p50_us": st["p50_us"], "p99_us": st["p99_us"], "p999_us": st["p999_us"],
-                      "per_instance_updates_per_s": [r["updates_per_s"] for r in res]}
+            total = 64
+            while total <= 16384:
+                pt = point(srv, ids, total)
                 sweep.append(pt)
-                if st["p99_us"] <= 1000.0 and (best is None or pt["updates_per_s"] > best["updates_per_s"]):
+                ok = pt["p99_us"] <= 1000.0
+                if ok and (best is None or pt["updates_per_s"] > best["updates_per_s"]):
                     best = pt
-                if st["p99_us"] > 1000.0 and per >= 4:
+                if per_update and not ok and best is None and total > len(insts):
+                    total //= 2          # the per-update path: find a load it sustains
+                    continue
+                if not ok:
                     break
-                per *= 2
+                if per_update and best is not None and len(sweep) > 1 and sweep[-2]["p99_us"] > 1000.0:
+                    break                # came down to a sustainable load
+                total *= 2
             for k in ids:
                 srv.detach(k)
         out[mode] = {"best_at_p99_le_1ms": best, "sweep": sweep}
-    ok = True
+    ok, ref_ok = True, True
     for i in insts:
         inc = i["g"].values()
         i["g"].build_tree(i["algo"], i["root"])
         ok &= bool(np.array_equal(inc, i["g"].values()))
         i["g"].close()
+        if i["scale"] <= 22 and not args.no_cpu_baseline:
+            n_add, n_del = (i["offset"] + 1) // 2, i["offset"] // 2
+            res, err = ref_driver("build", i["algo"], f"rmat:{i['scale']}:{i['scale']}@{n_del}:{i['imported'] + n_add}",
+                                  1 << i["scale"], i["root"], timeout=args.ref_timeout)
+            ref_ok = ref_ok and res is not None and bool(np.array_equal(res[1]["val"], inc))
     out["incremental_equals_rebuild"] = ok
+    out["values_match_reference"] = None if args.no_cpu_baseline else ref_ok
+    out["reference_checked_scales"] = [16, 18, 20, 22]
     b0, b1 = out["per_update"]["best_at_p99_le_1ms"], out["served"]["best_at_p99_le_1ms"]
     out["served_over_per_update"] = (b1["updates_per_s"] / b0["updates_per_s"]) if b0 and b1 else None
     return out
 
 
-def wcc_deletions(args):
+def leg_wcc_del(args):
     """Incremental WCC with heavy deletion: an undirected graph of 2^s vertices
     and 16 * 2^s edges (half uniform endpoints, half RMAT-s), both directions
     stored; the first 80% loaded; then batches of 1,000 updates (500 inserts of
     the next edges, 500 deletes of which half remove the oldest loaded edges and
     half remove current tree edges (a vertex's parent edge), forcing subtree
-    repair), each batch one rg_apply_add_del; min-vertex-id labels checked
-    against a rebuild at the end."""
+    repair), each batch one rg_apply_add_del.  The batches are recorded and
+    replayed through the reference: the value checksum after every batch must
+    match.  Min-vertex-id labels are also checked against a rebuild."""
     import ctypes
+
     import risgraph_b200 as rg
     from risgraph_b200 import gen
     scale = args.wcc_scale
@@ -422,7 +586,11 @@ def wcc_deletions(args):
 
     batch, half = 1000, 500
     nb = min(args.wcc_updates // batch, (E - imported) // half)
+    replay = scale <= args.wcc_ref_max_scale and not args.no_cpu_baseline
+    tmp = tempfile.mkdtemp(prefix="rg_wcc_")
+    bf = open(os.path.join(tmp, "batches.bin"), "wb") if replay else None
     ts, recomputes, invalidated = [], 0, 0
+    sums = np.zeros(nb, np.uint64)
     have = refresh()
     for k in range(nb):
         if k % 50 == 0 and k:
@@ -433,9 +601,14 @@ def wcc_deletions(args):
         vs = rng.choice(have, half // 2, replace=False) if len(have) >= half // 2 else have
         tree = np.stack([par[vs], vs.astype(np.uint64)], axis=1)
         dels = np.concatenate([old, tree]).astype(np.uint64)
+        if bf:
+            bf.write(np.array([len(adds), len(dels)], np.uint64).tobytes())
+            bf.write(np.ascontiguousarray(adds, np.uint64).tobytes())
+            bf.write(np.ascontiguousarray(dels, np.uint64).tobytes())
         t = time.perf_counter()
         g.apply_add_del("wcc", adds, dels, directed=False)
         ts.append(time.perf_counter() - t)
+        sums[k] = g.checksum()
         st = g.last_stats()
         recomputes += st["recomputes"]
         invalidated += st["invalidated"]
@@ -453,25 +626,64 @@ def wcc_deletions(args):
            "invalidated_per_batch": invalidated / max(nb, 1), "full_recomputes": recomputes,
            "incremental_equals_rebuild": ok}
     g.close()
+    del pairs
+    if bf:
+        bf.close()
+        res, err = ref_driver("replay", "wcc", f"mix:{scale}:{E}:{args.seed}", V, 0, imported,
+                              os.path.join(tmp, "batches.bin"), timeout=args.ref_timeout)
+        if res is None:
+            out["reference"] = {"unavailable": err}
+        else:
+            info, arr = res
+            out["checksums_match_reference"] = bool(np.array_equal(arr["sums"], sums))
+            out["values_match_reference"] = bool(np.array_equal(arr["val"], inc))
+            rt = np.asarray(info["times"])
+            out["reference"] = {"updates_per_s": batch * len(rt) / float(rt.sum()),
+                                "batch_p50_ms": float(np.percentile(rt, 50)) * 1e3, "cores": info["threads"],
+                                "kind": "reference", "sample": "the same batches, replayed"}
+    import shutil
+    shutil.rmtree(tmp, ignore_errors=True)
     return out
+
+
+# ---------------------------------------------------------------- main
+
+def max_over_ranks(x, dist):
+    """The slowest rank's time (every rank takes part; NCCL ranks reduce on
+    their GPU, gloo ranks on the CPU)."""
+    if not dist:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, world, seconds):
+    """Whole-job GTEPS of `world` independent replicas, each processing
+    units_per_rank edges, timed by the slowest rank."""
+    return units_per_rank * world / seconds / 1e9
+
+
+def single_leg(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    if args.wcc_deletions:
+        mode, res = "wcc_deletions", leg_wcc_del(args)
+    elif args.batch_sweep:
+        mode, res = "batch_sweep", leg_batches(args)
+    else:
+        mode, res = "served_mix", leg_served_mix(args)
+    print(json.dumps({"metric": METRIC, "mode": mode, "data": "synthetic", **res}))
 
 
 def main():
     args = parse()
-    if args.wcc_deletions:
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        if int(os.environ.get("RANK", "0")) == 0:
-            print(json.dumps({"metric": METRIC, "mode": "wcc_deletions", "data": "synthetic", **wcc_deletions(args)}))
-        return
-    if args.batch_sweep or args.served_mix:
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        if int(os.environ.get("RANK", "0")) == 0:
-            res = batch_sweep(args) if args.batch_sweep else served_mix(args)
-            print(json.dumps({"metric": METRIC, "mode": "batch_sweep" if args.batch_sweep else "served_mix",
-                              "data": "synthetic", **res}))
-        return
+    if args.wcc_deletions or args.batch_sweep or args.served_mix:
+        return single_leg(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -485,8 +697,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import risgraph_b200 as rg
+    from risgraph_b200 import gen
 
-    pairs, V, root = make_graph_input(args)
+    pairs = gen.rmat(args.scale, seed=args.seed)
+    V = 1 << args.scale
+    root = gen.max_out_degree_vertex(pairs, V)
     algo = args.algo
     directed = algo != "wcc"
     g = rg.Graph(V, len(pairs), symmetric=not directed, weighted=WEIGHTED[algo])
@@ -538,7 +753,14 @@ def main():
     assert np.array_equal(host_vals, values)
     e2e = replica_throughput(E_r * args.steps, world, e2e_s)
 
-    # roofline of the level kernels of one build (every level's mode kernels, timed per level)
+    # roofline: algorithmic bytes of one build over the device time per build of
+    # the timed region (the build's kernels, graph-launched, back to back)
+    ms_per_build = total_ms / args.steps
+    alg = algorithmic_bytes(V, V_r, E_r, algo)
+    peak, peak_kind = load_peaks()
+    achieved = alg / (ms_per_build / 1e3) / 1e9
+    # the level kernels alone, launched level by level with events around each
+    # level (profile mode): the share of the build spent in relaxation levels
     g.profile(True)
     g.profile_read()
     nb = 3
@@ -550,47 +772,81 @@ def main():
             torch.cuda.nvtx.range_pop()
     plaunch, pms = g.profile_read()
     g.profile(False)
-    push_ms_per_build = pms / nb
-    alg = algorithmic_bytes(V, V_r, E_r, algo)
-    peak, peak_kind = load_peaks()
-    achieved = alg / (push_ms_per_build / 1e3) / 1e9
     traffic, traffic_src = None, None
-    if algo == "sssp":
-        # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of every level kernel of one
-        # SSSP build, from an ncu capture of the RMAT-21 build (32,130,409 reached edges); the
-        # pull levels stream the in-edge copy, so the bytes grow with the reached edges
-        traffic = 1_497_410_816 * E_r / 32_130_409
-        traffic_src = "ncu capture of one RMAT-21 SSSP build, scaled by reached edges"
+    if algo == "sssp" and args.scale == 22:
+        # DRAM bytes of one build's level kernels, summed over one-kernel ncu captures
+        # (dram__bytes_read.sum + dram__bytes_write.sum), scaled by the reached edges
+        tr = os.path.join(ROOT, "profiles", "traffic_sssp_build.json")
+        if os.path.exists(tr):
+            d = json.load(open(tr))
+            traffic = d["bytes_per_build"] * E_r / d["E_r"]
+            traffic_src = d["source"]
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": traffic, "traffic_unit": "bytes per build",
             "traffic_source": traffic_src,
-            "kernel": "level kernels of one build (k_level_begin + the level mode's push/pull kernels, all levels)",
-            "algorithmic_bytes": alg, "launches_per_build": plaunch / nb, "kernel_ms_per_build": push_ms_per_build}
+            "kernel": "one build_tree: its init kernel and every level kernel, graph-launched, device time per "
+                      "build of the timed region",
+            "algorithmic_bytes": alg, "ms_per_build": ms_per_build,
+            "level_kernels_ms_per_build": pms / nb, "level_launches_per_build": plaunch / nb,
+            "level_kernels_note": "profile mode: the same level kernels launched level by level with events "
+                                  "around each level"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res, err = cpu_reference(pairs, V, root, algo, 2, 1, args.cpu_timeout)
+        res, err = ref_driver("build", algo, f"rmat:{args.scale}:{args.seed}", V, root, 2, 1,
+                              timeout=args.ref_timeout)
         if res is None:
-            cpu = {"value": None, "unit": "GTEPS", "cores": os.cpu_count(), "kind": "reference", "sample": err}
+            cpu = {"value": None, "unit": "GTEPS", "cores": ref_cores(), "kind": "reference", "sample": err}
         else:
-            info, vals = res
-            ok = bool(np.array_equal(vals, values))
+            info, arr = res
             t = float(np.mean(info["build_times"]))
             cpu = {"value": E_r / t / 1e9, "unit": "GTEPS", "cores": info["threads"], "kind": "reference",
                    "sample": f"RMAT-{args.scale} {algo} build_tree x2 after 1 warm-up "
-                             f"(load {info['load_s']:.1f}s untimed)", "values_match_gpu": ok}
-
+                             f"(generation and load {info['load_s']:.1f}s untimed)",
+                   "values_match_gpu": bool(np.array_equal(arr["val"], values))}
     g.close()
-    served = served_leg(args) if (rank == 0 and world == 1 and args.served_scale) else None
+    del pairs
+
+    legs = {}
+    want = [] if args.legs == "none" else [x for x in args.legs.split(",") if x]
+    if rank == 0 and world == 1:
+        fns = {"builds": lambda: leg_builds(args, peak), "bfs_inc": lambda: leg_bfs_inc(args),
+               "batches": lambda: leg_batches(args), "served": lambda: leg_served(args),
+               "served_mix": lambda: leg_served_mix(args), "wcc_del": lambda: leg_wcc_del(args)}
+        for name in want:
+            t = time.time()
+            print(f"[bench] leg {name} ...", file=sys.stderr, flush=True)
+            try:
+                legs[name] = fns[name]()
+            except Exception as e:  # noqa: BLE001 - one failed leg must not hide the others
+                legs[name] = {"error": repr(e)[-400:]}
+            legs[name]["leg_wall_s"] = time.time() - t
+            print(f"[bench] leg {name} done in {legs[name]['leg_wall_s']:.1f} s", file=sys.stderr, flush=True)
 
     if rank == 0:
+        parity = {"config2_" + algo: (cpu or {}).get("values_match_gpu")}
+        b = legs.get("builds", {})
+        for a in ("bfs", "sswp", "wcc"):
+            if a in b:
+                parity["config2_" + a] = b[a].get("values_match_reference")
+        if "bfs_inc" in legs:
+            parity["config1_bfs_inc"] = legs["bfs_inc"].get("checksums_match_reference")
+        for a, r in legs.get("batches", {}).get("runs", {}).items():
+            parity["config3_" + a] = r.get("checksums_match_reference")
+        if "served" in legs:
+            parity["served_rmat24"] = legs["served"].get("values_match_reference")
+        if "served_mix" in legs:
+            parity["config4_served_mix"] = legs["served_mix"].get("values_match_reference")
+        if "wcc_del" in legs:
+            parity["config5_wcc_del"] = legs["wcc_del"].get("checksums_match_reference")
         line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
                 "config": workload(args), "clocks": clk.summary(),
                 "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": V * 8},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "reached": {"V_r": V_r, "E_r": E_r}, "autotune": tune, "served": served}
+                "reached": {"V_r": V_r, "E_r": E_r}, "autotune": tune,
+                "parity_vs_reference": parity, **legs}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -15,10 +15,14 @@
  * core/graph.hpp:1728).  Distinct graphs may be used from distinct threads.
  * Every call returns after its device work has completed.
  *
- * Limits of the device layout: vertices < 2^31 and, for weighted graphs,
- * edge weights < 2^31 (the reference stores 48-bit ids and 64-bit weights);
- * edge multiplicities are 32-bit (the reference's are 16-bit,
- * core/type.hpp:24).  Out-of-range input returns an error, never a fault. */
+ * Limits of the device layout: vertices < 2^31 (the reference stores 48-bit
+ * ids, core/type.hpp:23); edge weights are uint64 as in the reference
+ * (core/type.hpp:25) below 2^64 - 2^27, where the reference's u64 sum
+ * value + weight would wrap around; edge multiplicities are 32-bit (the
+ * reference's are 16-bit, core/type.hpp:24).  Weights above 2^27 (the
+ * SSSP/SSWP sentinel) are kept on the device as 32-bit codes, which every
+ * hook compares exactly as the full weight, and read back in full.
+ * Out-of-range input returns an error, never a fault. */
 #ifndef RISGRAPH_B200_H
 #define RISGRAPH_B200_H
 #include <stddef.h>
@@ -34,7 +38,7 @@ typedef enum {
   RG_OK = 0,
   RG_EINVAL = 1,        /* bad argument (null graph, bad algorithm, size) */
   RG_EINVAL_VID = 2,    /* vertex id >= |V| */
-  RG_EINVAL_WEIGHT = 3, /* weight >= 2^31 on a weighted graph */
+  RG_EINVAL_WEIGHT = 3, /* weight >= 2^64 - 2^27 on a weighted graph */
   RG_ENOMEM_HBM = 4,    /* device allocation failed / HBM budget exceeded */
   RG_ENOSPACE = 5,      /* edge pool or edge index full */
   RG_ETIMEOUT = 6,      /* a bounded device wait gave up */
@@ -197,7 +201,12 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
  *                         invalidated set exceeds max(this, |V|/20)
  *   RG_OPT_PULL_SPLIT     pull levels run the longest in-lists in a first launch
  *                         so the rest read this level's hub values: 1 always,
- *                         0 never, 2 (default) for SSSP and WCC */
+ *                         0 never, 2 (default) for SSSP and WCC
+ *   RG_OPT_MAX_LEVELS     bound on the relaxation levels of one tree call
+ *                         (0, the default: 4 |V| + 1024).  A call that reaches
+ *                         it stops with RG_ETIMEOUT and leaves the labels
+ *                         partly updated; the graph stays usable and the next
+ *                         rg_build_tree restores them. */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -207,7 +216,8 @@ typedef enum {
   RG_OPT_BFS_BU_DIV = 5,
   RG_OPT_PULL_DIV = 6,
   RG_OPT_TINY_EDGES = 7,
-  RG_OPT_PULL_SPLIT = 8
+  RG_OPT_PULL_SPLIT = 8,
+  RG_OPT_MAX_LEVELS = 9
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);
@@ -241,17 +251,29 @@ int rg_device_bytes(rg_graph *g, uint64_t *bytes);
  *
  * Input: a CSR graph in caller-owned DEVICE memory: row_offsets[vertices+1]
  * (uint64, non-decreasing, last <= edges), columns[edges] (uint32 < vertices),
- * weights[edges] (uint32, or NULL for unweighted).  Output: values[vertices]
+ * weights[edges] (uint32; required for RG_SSSP and RG_SSWP, ignored for RG_BFS
+ * and RG_WCC; NULL with SSSP/SSWP is RG_EINVAL).  Output: values[vertices]
  * and parents[vertices] (parent == vertices for none) in caller-owned device
  * memory; either may be NULL, not both.  Runs on cuda_stream (NULL = default)
- * and returns when done.  No cudaMalloc/cudaFree or allocating library call:
- * the working memory is one static device array of about 28 MB, reserved on
- * every GPU that loads the library until exit, which bounds the graph to
- * RG_STATIC_MAX_VERTICES vertices (larger graphs: RG_EINVAL).  All calls share
- * that array: calls that overlap on the GPU race and give undefined results.
- * The first call on each device looks the array's address up (with that device
- * current); make it before any stream capture.  Malformed CSR input returns
- * RG_EINVAL / RG_EINVAL_VID without touching memory out of range. */
+ * and is synchronous: it reads a frontier count back to the host after every
+ * level and returns when the tree is written, so it must not be called on a
+ * stream that is being captured.  No cudaMalloc/cudaFree or allocating library
+ * call: the working memory is one static device array of about 28 MB, held by
+ * every GPU that loads the library's device code until exit, which bounds the
+ * graph to RG_STATIC_MAX_VERTICES vertices (larger graphs: RG_EINVAL).  All
+ * calls share that array: calls that overlap on the GPU race and give
+ * undefined results.
+ *
+ * Set-up: CUDA loads a library's device code lazily by default
+ * (CUDA_MODULE_LOADING=LAZY), so the 28 MB are only taken on a device when
+ * this library's device code is first used there.  The first call on each
+ * device (with that device current) looks the array's address up, which
+ * loads the module.  A caller whose memory is later claimed by a pool fixed at
+ * start-up should therefore make a set-up call at start-up, before the pool
+ * reserves its memory: vertices == 0 with every pointer NULL only does this
+ * per-device set-up and returns RG_OK (or run with CUDA_MODULE_LOADING=EAGER).
+ * Malformed CSR input returns RG_EINVAL / RG_EINVAL_VID without touching
+ * memory out of range. */
 #define RG_STATIC_MAX_VERTICES (1u << 20)
 int rg_build_tree_csr_static(int algo, uint64_t root, uint64_t vertices, uint64_t edges,
                              const uint64_t *row_offsets, const uint32_t *columns, const uint32_t *weights,

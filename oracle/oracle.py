@@ -184,24 +184,42 @@ def ref_available() -> bool:
     return os.path.exists(REF_DRIVER)
 
 
-def ref_run(mode: str, algo: str, pairs: np.ndarray, V: int, root: int, *args, threads: int | None = None,
-            workdir: str | None = None):
-    """Run the reference-built oracle on pairs; returns (json, dict of arrays)."""
+def ref_run(mode: str, algo: str, pairs, V: int, root, *args, threads: int | None = None,
+            workdir: str | None = None, timeout: float | None = None, bind: bool = False):
+    """Run the reference-built oracle; returns (json, dict of arrays).
+
+    `pairs` is an (n,2) uint64 array (written to a file in the reference's
+    binary format) or a graph spec string the driver generates itself
+    ("rmat:<scale>:<seed>", "mix:<scale>:<edges>:<seed>", optionally with an
+    "@<lo>:<hi>" window).  `root` may be "maxdeg".  threads = OpenMP threads
+    (all host cores when None); bind pins them (OMP_PROC_BIND=true)."""
+    own = workdir is None
     tmp = workdir or tempfile.mkdtemp(prefix="rgref_")
-    path = os.path.join(tmp, "g.bin")
-    np.ascontiguousarray(pairs, dtype=np.uint64).tofile(path)
-    out = os.path.join(tmp, "out")
-    cmd = [REF_DRIVER, mode, algo, path, str(V), str(root)] + [str(a) for a in args] + [out]
-    if mode == "build" and args:
-        cmd = [REF_DRIVER, mode, algo, path, str(V), str(root), out] + [str(a) for a in args]
-    env = dict(os.environ)
-    if threads:
-        env["OMP_NUM_THREADS"] = str(threads)
-    r = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
-    info = json.loads(r.stdout.strip().splitlines()[-1])
-    arrays = {}
-    for ext in ("val", "par", "pw", "sums"):
-        f = out + "." + ext
-        if os.path.exists(f):
-            arrays[ext] = np.fromfile(f, dtype=np.uint64)
-    return info, arrays
+    try:
+        if isinstance(pairs, str):
+            path = pairs
+        else:
+            path = os.path.join(tmp, "g.bin")
+            np.ascontiguousarray(pairs, dtype=np.uint64).tofile(path)
+        out = os.path.join(tmp, "out")
+        cmd = [REF_DRIVER, mode, algo, path, str(V), str(root)] + [str(a) for a in args] + [out]
+        if mode == "build" and args:
+            cmd = [REF_DRIVER, mode, algo, path, str(V), str(root), out] + [str(a) for a in args]
+        env = dict(os.environ)
+        env["OMP_NUM_THREADS"] = str(threads or os.cpu_count() or 1)
+        if bind:
+            env["OMP_PROC_BIND"] = "true"
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_driver {mode} {algo} failed ({r.returncode}): {r.stderr[-300:]}")
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        arrays = {}
+        for ext in ("val", "par", "pw", "sums"):
+            f = out + "." + ext
+            if os.path.exists(f):
+                arrays[ext] = np.fromfile(f, dtype=np.uint64)
+        return info, arrays
+    finally:
+        if own:
+            import shutil
+            shutil.rmtree(tmp, ignore_errors=True)

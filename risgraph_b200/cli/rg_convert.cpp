@@ -6,10 +6,14 @@
 //   convert_to_binary_random     < "src dst" lines  > graph.bin   (shuffled)
 //   convert_to_binary_timestamp  < "src dst t" lines > graph.bin  (sorted by t, then src, dst)
 //
-// The shuffle is a seeded Fisher-Yates (RG_SHUFFLE_SEED, default 1) rather than
-// std::random_shuffle's unspecified generator, so a shuffled file can be
-// produced again.  Input is read in large blocks; any run of characters other
-// than digits separates numbers, as with scanf("%lu").
+// Without RG_SHUFFLE_SEED the shuffle is std::random_shuffle over the
+// (src, dst) pairs with the C library's default rand() state, as
+// utils/convert_to_binary_random.cpp:28 does, so on the same C++ library the
+// output is byte-identical to the reference's.  With RG_SHUFFLE_SEED set it is
+// a Fisher-Yates shuffle driven by splitmix64 from that seed, which gives the
+// same file on every platform.  Input is read in large blocks; any run of
+// characters other than digits separates numbers (scanf("%lu") would also
+// take a sign).
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -96,9 +100,16 @@ int main(int argc, char **argv) {
     p.push_back(s);
     p.push_back(d);
   }
-  if (random) {
-    const char *env = std::getenv("RG_SHUFFLE_SEED");
-    uint64_t state = env ? std::strtoull(env, nullptr, 10) : 1;
+  if (random && !std::getenv("RG_SHUFFLE_SEED")) {
+    std::vector<std::pair<uint64_t, uint64_t>> e(p.size() / 2);
+    for (size_t i = 0; i < e.size(); i++) e[i] = {p[2 * i], p[2 * i + 1]};
+    std::random_shuffle(e.begin(), e.end());
+    for (size_t i = 0; i < e.size(); i++) {
+      p[2 * i] = e[i].first;
+      p[2 * i + 1] = e[i].second;
+    }
+  } else if (random) {
+    uint64_t state = std::strtoull(std::getenv("RG_SHUFFLE_SEED"), nullptr, 10);
     const size_t n = p.size() / 2;
     for (size_t i = n; i > 1; i--) {
       state = rg_gen_splitmix64(state);

@@ -50,12 +50,49 @@ int check_edges(const Graph &g, const rg_edge *edges, const uint64_t *pairs, uin
       rg::set_error("VertexId error.");  // core/graph.hpp:205,231
       return RG_EINVAL_VID;
     }
-    if (!pairs && g.weighted && edges[i].data >= (1ull << 31)) {
-      rg::set_error("edge weight >= 2^31");
+    if (!pairs && g.weighted && edges[i].data >= rg::W_LIMIT) {
+      rg::set_error("edge weight >= 2^64 - 2^27 (the reference's u64 sums would wrap)");
       return RG_EINVAL_WEIGHT;
     }
   }
   return RG_OK;
+}
+
+// The edges as the device takes them: weights above W_RAW_MAX replaced by
+// their codes (assigned on first sight), in `buf`; the input itself when no
+// weight needs a code (the common case costs one scan).
+int device_edges(Graph &g, const rg_edge *edges, uint64_t n, std::vector<rg_edge> &buf, const rg_edge **out) {
+  *out = edges;
+  if (!g.weighted || !edges) return RG_OK;
+  uint64_t i = 0;
+  while (i < n && edges[i].data <= rg::W_RAW_MAX) i++;
+  if (i == n) return RG_OK;
+  buf.assign(edges, edges + n);
+  std::lock_guard<std::mutex> lk(g.wmu);
+  for (; i < n; i++) {
+    uint64_t w = buf[i].data;
+    if (w <= rg::W_RAW_MAX) continue;
+    auto it = g.wcode.find(w);
+    if (it == g.wcode.end()) {
+      if (rg::W_CODE_BASE + g.wfull.size() >= rg::W_CODE_END) {
+        rg::set_error("more than 2^31 - 2^27 distinct edge weights above 2^27");
+        return RG_ENOSPACE;
+      }
+      it = g.wcode.emplace(w, (uint32_t)(rg::W_CODE_BASE + g.wfull.size())).first;
+      g.wfull.push_back(w);
+    }
+    buf[i].data = it->second;
+  }
+  *out = buf.data();
+  return RG_OK;
+}
+
+// Parent weights read back: codes to full weights.
+void host_weights(Graph &g, uint64_t *w, uint64_t n) {
+  std::lock_guard<std::mutex> lk(g.wmu);
+  if (g.wfull.empty()) return;
+  for (uint64_t i = 0; i < n; i++)
+    if (w[i] >= rg::W_CODE_BASE && w[i] - rg::W_CODE_BASE < g.wfull.size()) w[i] = g.wfull[w[i] - rg::W_CODE_BASE];
 }
 
 int check_algo(const Graph &g, int algo) {
@@ -77,6 +114,8 @@ int edge_updates(rg_graph *gh, const rg_edge *edges, const uint64_t *pairs, uint
   Graph &g = gh->g;
   int rc = check_edges(g, edges, pairs, n);
   if (rc) return rc;
+  std::vector<rg_edge> wbuf;
+  if ((rc = device_edges(g, edges, n, wbuf, &edges))) return rc;
   // small batches (single updates, served epochs): one fused graph launch
   if (apply && n && n <= rg::SMALL_EDGES && !g.profiling) return rg::apply_small(g, edges, pairs, n, directed, add, old_num);
   const int what = add ? 1 : 2;
@@ -111,6 +150,8 @@ int tree_updates(rg_graph *gh, int algo, const rg_edge *edges, uint64_t n, int d
   int rc = check_algo(g, algo);
   if (rc) return rc;
   if ((rc = check_edges(g, edges, nullptr, n))) return rc;
+  std::vector<rg_edge> wbuf;
+  if ((rc = device_edges(g, edges, n, wbuf, &edges))) return rc;
   uint64_t sum = 0;
   for (uint64_t b = 0; b < n; b += CHUNK_EDGES) {
     uint64_t m = std::min(CHUNK_EDGES, n - b), nops = 0, t = 0;
@@ -258,8 +299,14 @@ int rg_apply_add_del(rg_graph *g, int algo, const rg_edge *adds, uint64_t n_add,
   if (!rc) rc = check_edges(g->g, adds, nullptr, n_add);
   if (!rc) rc = check_edges(g->g, dels, nullptr, n_del);
   if (rc) return rc;
-  if (n_add && n_del && n_add <= rg::SMALL_EDGES && n_del <= rg::SMALL_EDGES && !g->g.profiling)
-    return rg::apply_add_del_small(g->g, adds, n_add, dels, n_del, directed);
+  if (n_add && n_del && n_add <= rg::SMALL_EDGES && n_del <= rg::SMALL_EDGES && !g->g.profiling) {
+    std::vector<rg_edge> abuf, dbuf;
+    const rg_edge *a = adds, *d = dels;
+    if (!rc) rc = device_edges(g->g, adds, n_add, abuf, &a);
+    if (!rc) rc = device_edges(g->g, dels, n_del, dbuf, &d);
+    return rc ? rc : rg::apply_add_del_small(g->g, a, n_add, d, n_del, directed);
+  }
+  // (edge_updates codes the weights itself)
   rc = edge_updates(g, adds, nullptr, n_add, directed, nullptr, true, true);
   return rc ? rc : edge_updates(g, dels, nullptr, n_del, directed, nullptr, false, true);
 }
@@ -282,6 +329,8 @@ int rg_get_edge_num(rg_graph *gh, const rg_edge *edges, uint64_t n, uint64_t *nu
   Graph &g = gh->g;
   if ((rc = check_edges(g, edges, nullptr, n))) return rc;
   if (!num) { rg::set_error("null output"); return RG_EINVAL; }
+  std::vector<rg_edge> wbuf;
+  if ((rc = device_edges(g, edges, n, wbuf, &edges))) return rc;
   for (uint64_t b = 0; b < n; b += CHUNK_EDGES) {
     uint64_t m = std::min(CHUNK_EDGES, n - b), nops = 0;
     if ((rc = rg::stage_edges(g, edges + b, nullptr, m, 1, &nops))) return rc;
@@ -327,6 +376,8 @@ int rg_classify(rg_graph *gh, int algo, const rg_edge *edges, const uint8_t *is_
   if ((rc = check_algo(g, algo))) return rc;
   if ((rc = check_edges(g, edges, nullptr, n))) return rc;
   if (!unsafe) { rg::set_error("null output"); return RG_EINVAL; }
+  std::vector<rg_edge> wbuf;
+  if ((rc = device_edges(g, edges, n, wbuf, &edges))) return rc;
   for (uint64_t b = 0; b < n; b += CHUNK_EDGES) {
     uint64_t m = std::min(CHUNK_EDGES, n - b), nops = 0;
     if ((rc = rg::stage_edges(g, edges + b, nullptr, m, directed, &nops))) return rc;
@@ -347,7 +398,9 @@ int rg_classify(rg_graph *gh, int algo, const rg_edge *edges, const uint8_t *is_
 
 int rg_get_labels(rg_graph *gh, uint64_t *value, uint64_t *parent, uint64_t *parent_w) {
   int rc = check_graph(gh);
-  return rc ? rc : rg::tree_labels(gh->g, value, parent, parent_w);
+  if (!rc) rc = rg::tree_labels(gh->g, value, parent, parent_w);
+  if (!rc && parent_w && gh->g.weighted) host_weights(gh->g, parent_w, gh->g.V);
+  return rc;
 }
 
 int rg_get_modified(rg_graph *gh, uint64_t *vids, uint64_t cap, uint64_t *n) {
@@ -515,6 +568,7 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
       if (value > 2) break;
       g.pull_split = (int)value;
       return RG_OK;
+    case RG_OPT_MAX_LEVELS: g.max_levels = value; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -533,6 +587,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_PULL_DIV: *value = g.pull_div; return RG_OK;
     case RG_OPT_TINY_EDGES: *value = g.tiny_edges; return RG_OK;
     case RG_OPT_PULL_SPLIT: *value = (uint64_t)g.pull_split; return RG_OK;
+    case RG_OPT_MAX_LEVELS: *value = g.max_levels; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

@@ -22,7 +22,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "risgraph_b200.h"
@@ -64,6 +66,7 @@ enum Ctl : int {
   C_INVTAG = 23,   // invalidation tag of the current deletion repair (tag+1 = rescued)
   C_INVITER = 24,  // invalidation levels run by the current deletion repair
   C_ROOT = 25,     // root of the label set (init_label_func argument)
+  C_HOSTCOND = 26, // a loop condition for the host, when profile mode steps a loop from the host
   C_COUNT = 32
 };
 
@@ -298,6 +301,7 @@ struct Graph {
   uint64_t adj_version = 1, pull_version = 0;
   int dense_pull = 2;  // dense build levels: 1 = pull over in-edges, 0 = edge-centric push, 2 = pull for WCC only
   uint64_t dense_div = 20, lbs_min = 2048, recompute_min = 2000000;
+  uint64_t max_levels = 0;  // bound on the levels of one tree call (0: 4 |V| + 1024)
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
@@ -323,7 +327,25 @@ struct Graph {
   cudaEvent_t pev[2] = {nullptr, nullptr};
   uint64_t prof_launches = 0;
   double prof_ms = 0.0;
+  // weights above W_RAW_MAX travel as 32-bit codes (see weight_code): code -> weight
+  std::mutex wmu;
+  std::unordered_map<uint64_t, uint32_t> wcode;
+  std::vector<uint64_t> wfull;
 };
+
+// Edge weights on the device are 32-bit.  A weight above W_RAW_MAX = 2^27 (the
+// SSSP/SSWP sentinel MAXL, src/sssp.cpp:66) can never lower an SSSP value
+// (s + w >= 2^27 >= d for every label d) and never limits an SSWP value
+// (min(s, w) = s, since s <= 2^27), so its exact size only matters to read it
+// back: such weights are exchanged on the host for distinct codes in
+// (2^27, 2^31), every comparison the hooks make gives the same answer, equal
+// weights stay one edge and different ones stay different edges, and
+// rg_get_labels turns a parent's code back into its full weight.  Weights at or
+// above W_LIMIT = 2^64 - 2^27 are refused: there the reference's u64 sum s + w
+// wraps around (a negative weight).
+constexpr uint64_t W_RAW_MAX = 1ull << 27;
+constexpr uint64_t W_CODE_BASE = W_RAW_MAX + 1, W_CODE_END = 1ull << 31;
+constexpr uint64_t W_LIMIT = 0ull - (1ull << 27);
 
 // Kernel launch bookkeeping (every launch site calls count_launch).
 inline void count_launch(Graph &g, int n = 1) { g.launches += (uint64_t)n; }

@@ -194,8 +194,8 @@ int check_request(const Instance &in, const rg_request &r) {
     rg::set_error("VertexId error.");
     return RG_EINVAL_VID;
   }
-  if (g.weighted && r.data >= (1ull << 31)) {
-    rg::set_error("edge weight >= 2^31");
+  if (g.weighted && r.data >= rg::W_LIMIT) {
+    rg::set_error("edge weight >= 2^64 - 2^27 (the reference's u64 sums would wrap)");
     return RG_EINVAL_WEIGHT;
   }
   return RG_OK;

@@ -13,15 +13,21 @@
 // Limits and sharing rules:
 //  * at most RG_STATIC_MAX_VERTICES vertices (larger graphs are rejected with
 //    RG_EINVAL before anything runs);
-//  * the scratch array (about 28 MB) is reserved on every GPU that loads the
-//    library, for the life of the process;
+//  * the scratch array (about 28 MB) is held on every GPU where this library's
+//    device code has been loaded, for the life of the process;
 //  * every call shares that one array, and it keeps the previous call's
 //    contents: each call clears the parts that must start at zero itself, but
 //    two calls whose work overlaps on the GPU (different streams, or different
 //    host threads) race on it and both results are undefined;
 //  * the device address of the array is looked up once per device, on the
-//    first call made with that device current (cudaGetSymbolAddress); make
-//    that first call before any stream capture begins.
+//    first call made with that device current (cudaGetSymbolAddress).  With
+//    lazy module loading (the CUDA default) that lookup is also what loads this
+//    library's device code, and with it the array, onto the device; a call
+//    with vertices == 0 and all pointers NULL does only this set-up, so that a
+//    caller can take the array at start-up, before another pool claims the
+//    device's memory;
+//  * each call is synchronous (a counter read-back per level) and must not be
+//    made on a stream under capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -204,6 +210,11 @@ extern "C" int rg_build_tree_csr_static(int algo, uint64_t root, uint64_t vertic
                                         const uint32_t *weights, uint64_t *values, uint64_t *parents,
                                         void *cuda_stream) {
   using namespace rg;
+  if (vertices == 0 && !row_offsets && !columns && !weights && !values && !parents) {
+    // set-up only: load the module and look the array's address up on this device
+    unsigned long long *base = nullptr;
+    return scratch_address(&base);
+  }
   if (vertices == 0 || vertices > RG_STATIC_MAX_VERTICES) {
     set_error("rg_build_tree_csr_static: vertices must be in [1, RG_STATIC_MAX_VERTICES]");
     return RG_EINVAL;
@@ -212,21 +223,20 @@ extern "C" int rg_build_tree_csr_static(int algo, uint64_t root, uint64_t vertic
     set_error("rg_build_tree_csr_static: null CSR or output pointer");
     return RG_EINVAL;
   }
+  if ((algo == RG_SSSP || algo == RG_SSWP) && !weights) {
+    set_error("rg_build_tree_csr_static: SSSP and SSWP need edge weights");
+    return RG_EINVAL;
+  }
   if (algo != RG_WCC && root >= vertices) {
     set_error("VertexId error.");
     return RG_EINVAL_VID;
   }
   cudaStream_t st = (cudaStream_t)cuda_stream;
-  const bool w = weights != nullptr;
   const uint64_t V = vertices, E = edges;
   switch (algo) {
     case RG_BFS: return run<RG_BFS, false>(V, E, root, row_offsets, columns, nullptr, values, parents, st);
-    case RG_SSSP:
-      return w ? run<RG_SSSP, true>(V, E, root, row_offsets, columns, weights, values, parents, st)
-               : run<RG_SSSP, false>(V, E, root, row_offsets, columns, nullptr, values, parents, st);
-    case RG_SSWP:
-      return w ? run<RG_SSWP, true>(V, E, root, row_offsets, columns, weights, values, parents, st)
-               : run<RG_SSWP, false>(V, E, root, row_offsets, columns, nullptr, values, parents, st);
+    case RG_SSSP: return run<RG_SSSP, true>(V, E, root, row_offsets, columns, weights, values, parents, st);
+    case RG_SSWP: return run<RG_SSWP, true>(V, E, root, row_offsets, columns, weights, values, parents, st);
     case RG_WCC: return run<RG_WCC, false>(V, E, 0, row_offsets, columns, nullptr, values, parents, st);
   }
   set_error("unknown algorithm");

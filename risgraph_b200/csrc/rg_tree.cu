@@ -1122,6 +1122,7 @@ struct LevelCfg {
   uint64_t pull_div;  // builds pull once frontier * pull_div >= |V|
   uint64_t pull_split;  // pull levels run in two launches
   uint64_t tiny_edges;
+  uint64_t max_levels;  // level bound baked into the loop graphs
   int allow_pull;
   int bottom_up;
 };
@@ -1197,12 +1198,16 @@ __global__ void k_inv_begin(DevGraph g, const unsigned long long *fin_n, unsigne
   c[C_INVITER] = it + 1;
 }
 
+// in_graph = 0: launched by the host (profile mode); the condition goes to
+// C_HOSTCOND instead of the WHILE node's handle.
 __global__ void k_inv_cond(DevGraph g, const unsigned long long *n_after, uint64_t max_iter,
-                           cudaGraphConditionalHandle handle) {
+                           cudaGraphConditionalHandle handle, int in_graph) {
   unsigned long long *c = g.ctl;
   const uint64_t n = *n_after;
   c[C_KLAUNCH] += 1;
-  cudaGraphSetConditional(handle, (n && !c[C_RECOMPUTE] && c[C_INVITER] < max_iter) ? 1u : 0u);
+  const unsigned go = (n && !c[C_RECOMPUTE] && c[C_INVITER] < max_iter) ? 1u : 0u;
+  if (in_graph) cudaGraphSetConditional(handle, go);
+  else c[C_HOSTCOND] = go;
 }
 
 __global__ void k_copy_frontier(DevGraph g, const uint32_t *src, const unsigned long long *src_n, uint32_t *dst,
@@ -1604,10 +1609,12 @@ __global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, c
 constexpr int DT_TPB = 1024;
 constexpr uint64_t DEL_TINY_N = 1024, DEL_TINY_TREE = 8192;
 
+// in_graph = 0: launched by the host (profile mode); the hand-over decision
+// goes to C_HOSTCOND instead of the IF node's handle.
 template <int A, bool W>
 __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, uint32_t *q1, uint32_t *tree,
                                                      uint64_t limit, uint64_t big, uint64_t max_iter, uint32_t mst,
-                                                     cudaGraphConditionalHandle standard) {
+                                                     cudaGraphConditionalHandle standard, int in_graph) {
   __shared__ int s_go;
   unsigned long long *c = g.ctl;
   const unsigned tid = threadIdx.x;
@@ -1661,7 +1668,8 @@ __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, u
     }
     if (tid == 0) {
       c[C_KLAUNCH] += 1;
-      cudaGraphSetConditional(standard, 1u);
+      if (in_graph) cudaGraphSetConditional(standard, 1u);
+      else c[C_HOSTCOND] = 1;
     }
     return;
   }
@@ -1682,7 +1690,8 @@ __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, u
   warp_add_result(local, &c[C_RESULT]);
   if (tid == 0) {
     c[C_KLAUNCH] += 1;
-    cudaGraphSetConditional(standard, 0u);
+    if (in_graph) cudaGraphSetConditional(standard, 0u);
+    else c[C_HOSTCOND] = 0;
   }
 }
 
@@ -1900,7 +1909,7 @@ int prepare_pull(Graph &g) {
   return g.weighted ? prepare_pull_w<true>(g) : prepare_pull_w<false>(g);
 }
 
-uint64_t max_levels_of(const Graph &g) { return 4 * (uint64_t)g.V + 1024; }
+uint64_t max_levels_of(const Graph &g) { return g.max_levels ? g.max_levels : 4 * (uint64_t)g.V + 1024; }
 
 // Kernels of one level mode for one half-level (queue half -> queue half^1).
 template <int A, bool W>
@@ -1963,6 +1972,7 @@ uint64_t cfg_key(const LevelCfg &c) {
   h = splitmix64(h ^ c.pull_div);
   h = splitmix64(h ^ c.pull_split);
   h = splitmix64(h ^ c.tiny_edges);
+  h = splitmix64(h ^ c.max_levels);
   return splitmix64(h ^ ((uint64_t)c.allow_pull << 1) ^ (uint64_t)c.bottom_up);
 }
 
@@ -1976,6 +1986,7 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   cfg.pull_div = g.pull_div;
   cfg.pull_split = pull_split_on(g, A) ? 1 : 0;
   cfg.tiny_edges = g.tiny_edges < TINY_EDGES ? g.tiny_edges : TINY_EDGES;
+  cfg.max_levels = max_levels_of(g);
   return cfg;
 }
 
@@ -2081,8 +2092,9 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
     if ((e = cudaGraphConditionalHandleCreate(&th, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) break;
     uint32_t *q0 = g.q[0], *q1 = g.q[1], *tr = g.tree;
     uint64_t max_iter = (uint64_t)g.V + 2;
+    int in_graph = 1;
     void *ta[] = {(void *)&g.d, (void *)&q0, (void *)&q1, (void *)&tr, (void *)&limit, (void *)&big,
-                  (void *)&max_iter, (void *)&mst, (void *)&th};
+                  (void *)&max_iter, (void *)&mst, (void *)&th, (void *)&in_graph};
     cudaKernelNodeParams tp = {};
     tp.func = (void *)k_del_tiny<A, W>;
     tp.gridDim = dim3(1);
@@ -2118,7 +2130,7 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
       k_rescue<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, limit);
       k_expand<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
     }
-    k_inv_cond<<<1, 1, 0, g.cap_stream>>>(g.d, &g.d.ctl[C_QN0], (uint64_t)g.V + 2, wh);
+    k_inv_cond<<<1, 1, 0, g.cap_stream>>>(g.d, &g.d.ctl[C_QN0], (uint64_t)g.V + 2, wh, 1);
     if ((e = cudaStreamEndCapture(g.cap_stream, &body)) != cudaSuccess) break;
     // k_reset -> k_pull -> k_copy_frontier after the loop
     unsigned long long *tree_n = &g.d.ctl[C_TREEN], *q0_n = &g.d.ctl[C_QN0];
@@ -2253,6 +2265,50 @@ int del_exec(Graph &g, cudaGraphExec_t *out) {
   return RG_OK;
 }
 
+// The deletion repair of add_del_repair launched kernel by kernel from the
+// host (profile mode): the same kernels in the same order, with the IF and
+// WHILE decisions read back through C_HOSTCOND, so that every kernel is a
+// plain launch a profiler lists.
+template <int A, bool W>
+int del_repair_stepped(Graph &g) {
+  const uint64_t big = recompute_threshold(g);
+  const uint64_t limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
+  const uint32_t mst = mod_stamp(g);
+  const int gridw = g.num_sms * 16;
+  const uint64_t max_iter = (uint64_t)g.V + 2;
+  count_launch(g);
+  k_del_tiny<A, W><<<1, DT_TPB, 0, g.stream>>>(g.d, g.q[0], g.q[1], g.tree, limit, big, max_iter, mst,
+                                               cudaGraphConditionalHandle{}, 0);
+  RG_CUDA(cudaGetLastError());
+  int rc = read_ctl(g);
+  if (rc) return rc;
+  if (!g.h_ctl[C_HOSTCOND]) return RG_OK;
+  for (uint64_t it = 0;; it++) {
+    if (it > max_iter) {
+      set_error("deletion repair did not converge");
+      return RG_ETIMEOUT;
+    }
+    for (int half = 0; half < 2; half++) {
+      unsigned long long *fin_n = &g.d.ctl[C_QN0 + half], *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
+      count_launch(g, 3);
+      k_inv_begin<<<1, 1, 0, g.stream>>>(g.d, fin_n, fout_n, big);
+      k_rescue<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.q[half], fin_n, limit);
+      k_expand<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
+    }
+    count_launch(g);
+    k_inv_cond<<<1, 1, 0, g.stream>>>(g.d, &g.d.ctl[C_QN0], max_iter, cudaGraphConditionalHandle{}, 0);
+    RG_CUDA(cudaGetLastError());
+    if ((rc = read_ctl(g))) return rc;
+    if (!g.h_ctl[C_HOSTCOND]) break;
+  }
+  count_launch(g, 3);
+  k_reset<A><<<gridw, TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
+  k_pull<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
+  k_copy_frontier<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], g.q[0], &g.d.ctl[C_QN0]);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
+}
+
 template <int A, bool W>
 int build_enqueue(Graph &g, uint64_t root) {
   int rc = guard_counters(g);
@@ -2292,9 +2348,14 @@ int del_enqueue(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
       g.d, op_src(g), op_dst(g), op_w(g), from_cands ? op_cand(g) : nullptr, &g.d.ctl[C_CANDN], n_edges, directed,
       g.q[0], &g.d.ctl[C_QN0]);
   RG_CUDA(cudaGetLastError());
-  cudaGraphExec_t exec;
-  if ((rc = del_exec<A, W>(g, &exec))) return rc;
-  RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  if (g.profiling) {
+    rc = del_repair_stepped<A, W>(g);
+  } else {
+    cudaGraphExec_t exec;
+    if ((rc = del_exec<A, W>(g, &exec))) return rc;
+    RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  }
+  if (rc) return rc;
   return push_levels<A, W>(g, false);
 }
 

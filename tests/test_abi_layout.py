@@ -76,7 +76,8 @@ def test_option_names_match_header_enum():
     # every Python name maps to the header's value of the same knob
     names = {"dense_pull": "DENSE_PULL", "dense_div": "DENSE_DIV", "lbs_min": "LBS_MIN",
              "bfs_bottom_up": "BFS_BOTTOM_UP", "recompute_min": "RECOMPUTE_MIN", "bu_div": "BFS_BU_DIV",
-             "pull_div": "PULL_DIV", "tiny_edges": "TINY_EDGES", "pull_split": "PULL_SPLIT"}
+             "pull_div": "PULL_DIV", "tiny_edges": "TINY_EDGES", "pull_split": "PULL_SPLIT",
+             "max_levels": "MAX_LEVELS"}
     assert set(py) == set(names), set(py) ^ set(names)
     for k, v in py.items():
         assert header[names[k]] == v, k

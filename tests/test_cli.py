@@ -128,6 +128,9 @@ def test_converters(tmp_path):
         return np.frombuffer(r.stdout, dtype=np.uint64).reshape(-1, 2)
 
     np.testing.assert_array_equal(conv("convert_to_binary", txt), edges)
+    u = conv("convert_to_binary_random", txt)
+    np.testing.assert_array_equal(u, conv("convert_to_binary_random", txt))  # rand()'s default state
+    np.testing.assert_array_equal(np.sort(u.view("u8,u8"), axis=0), np.sort(edges.view("u8,u8"), axis=0))
     a = conv("convert_to_binary_random", txt, {"RG_SHUFFLE_SEED": "7"})
     b = conv("convert_to_binary_random", txt, {"RG_SHUFFLE_SEED": "7"})
     np.testing.assert_array_equal(a, b)  # seeded: reproducible
@@ -135,3 +138,29 @@ def test_converters(tmp_path):
     np.testing.assert_array_equal(np.sort(a.view("u8,u8"), axis=0), np.sort(edges.view("u8,u8"), axis=0))
     order = sorted(range(500), key=lambda i: (int(ts[i]), int(edges[i, 0]), int(edges[i, 1])))
     np.testing.assert_array_equal(conv("convert_to_binary_timestamp", txt_t), edges[order])
+
+
+REF_BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_BIN, "convert_to_binary_random")),
+                    reason="reference converters not built (oracle/ref/build_ref.sh)")
+def test_converters_byte_identical_to_reference(tmp_path):
+    """The three converters against the reference's own (utils/convert_to_binary*.cpp,
+    compiled unmodified into oracle/_ref): byte-identical output on the same
+    input, the unseeded shuffle included (std::random_shuffle, rand()'s default
+    state), with duplicates and a timestamp order with ties."""
+    rng = np.random.default_rng(11)
+    edges = rng.integers(0, 1 << 36, size=(3000, 2), dtype=np.uint64)
+    edges[100:200] = edges[0:100]                      # duplicate edges
+    ts = rng.integers(0, 40, size=3000, dtype=np.uint64)
+    texts = {"convert_to_binary": "\n".join(f"{s} {d}" for s, d in edges.tolist()) + "\n",
+             "convert_to_binary_timestamp": "\n".join(f"{s} {d} {t}" for (s, d), t in
+                                                      zip(edges.tolist(), ts.tolist())) + "\n"}
+    texts["convert_to_binary_random"] = texts["convert_to_binary"]
+    for name, text in texts.items():
+        ours = subprocess.run([os.path.join(BIN, name)], input=text.encode(), capture_output=True, timeout=60)
+        ref = subprocess.run([os.path.join(REF_BIN, name)], input=text.encode(), capture_output=True, timeout=60)
+        assert ours.returncode == 0 and ref.returncode == 0
+        assert len(ref.stdout) == 16 * len(edges)
+        assert ours.stdout == ref.stdout, name

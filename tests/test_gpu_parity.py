@@ -10,6 +10,7 @@ import risgraph_b200 as rg
 from risgraph_b200 import gen
 
 from helpers import ALGOS, WEIGHTED, edges_of, gpu_graph, oracle_graph
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -195,8 +196,9 @@ def test_bfs_inc_rmat16_10k_steps():
     1,048,576 edges), the first 90% loaded, root 0, then 10,000 sliding-window
     steps (insert raw[i], delete raw[i - imported]), each repaired at once;
     the depth of every vertex is compared after every step through the
-    value checksum: against the reference-built driver when it is present,
-    and against the oracle port."""
+    value checksum: against the reference-built driver (required: a GPU run
+    without oracle/_ref/ref_driver fails here rather than falling back) and
+    against the oracle port."""
     scale, steps = 16, 10000
     pairs = gen.rmat(scale, seed=16)
     V = 1 << scale
@@ -208,9 +210,9 @@ def test_bfs_inc_rmat16_10k_steps():
     ref = og.run_inc(pairs, imported, steps, 0)
     assert len(ref) == steps
     from oracle import oracle as O
-    if O.ref_available():
-        _, arrays = O.ref_run("inc", "bfs", pairs, V, 0, 0.9, steps)
-        np.testing.assert_array_equal(arrays["sums"][:steps], ref)
+    assert O.ref_available(), "oracle/_ref/ref_driver is missing: build it with oracle/ref/build_ref.sh"
+    _, arrays = O.ref_run("inc", "bfs", pairs, V, 0, 0.9, steps)
+    np.testing.assert_array_equal(arrays["sums"][:steps], ref)
     sums = np.zeros(steps, np.uint64)
     for k in range(steps):
         i = imported + k
@@ -363,8 +365,12 @@ def test_errors_are_status_codes():
     with pytest.raises(rg.RGError) as ei:
         g.add_edge(5, 100, 3)
     assert ei.value.status == 2
+    # weights are uint64 as in the reference (core/type.hpp:25) below 2^64 - 2^27,
+    # where the reference's u64 sum value + weight would wrap
+    assert g.add_edge(5, 6, 1 << 31) == 0
+    assert g.add_edge(5, 7, (1 << 64) - (1 << 27) - 1) == 0
     with pytest.raises(rg.RGError) as ei:
-        g.add_edge(5, 6, 1 << 31)
+        g.add_edge(5, 6, (1 << 64) - (1 << 27))
     assert ei.value.status == 3
     with pytest.raises(rg.RGError) as ei:
         g.update_tree_add("sssp", [(1, 2, 3)])
@@ -377,6 +383,58 @@ def test_errors_are_status_codes():
     assert g.update_tree_add("sssp", np.zeros(0, rg.EDGE_DTYPE)) == 0
     assert g.update_tree_del("sssp", np.zeros(0, rg.EDGE_DTYPE)) == 0
     g.apply_add("sssp", np.zeros(0, rg.EDGE_DTYPE))
+
+
+@pytest.mark.parametrize("algo", ["sssp", "sswp"])
+def test_full_width_weights_vs_oracle(algo):
+    """uint64 weights (core/type.hpp:25): a fifth of the edges carry weights in
+    (2^27, 2^64 - 2^27), some of them parallel edges that differ only in a large
+    weight.  Build, a batch of inserts and a batch of deletes (one copy of each
+    parallel pair among them) give the oracle's values; every parent weight
+    reads back in full, and multiplicities are those of distinct weights."""
+    scale = 12
+    pairs = gen.rmat(scale, seed=71)
+    V = 1 << scale
+    rng = np.random.default_rng(71)
+    e = gen.edges_with_weights(pairs, True)
+    big = rng.random(len(e)) < 0.2
+    choices = np.array([(1 << 27) + 1, (1 << 31) + 5, (1 << 32) + 7, 1 << 40, (1 << 63) + 3,
+                        (1 << 64) - (1 << 27) - 1], dtype=np.uint64)
+    e["data"][big] = rng.choice(choices, int(big.sum()))
+    # parallel edges: the same endpoints with a second, different large weight
+    par_e = e[big][:300].copy()
+    par_e["data"] = np.where(par_e["data"] == choices[3], choices[4], choices[3])
+    imported = int(len(e) * 0.9)
+    load = np.concatenate([e[:imported], par_e])
+    g = rg.Graph(V, len(e) + len(par_e), weighted=True)
+    g.add_edges(load)
+    og = O.OracleGraph(algo, V, len(e) + len(par_e))
+    for x in load:
+        og.add_edge(int(x["src"]), int(x["dst"]), int(x["data"]))
+    root = gen.max_out_degree_vertex(pairs, V)
+    g.build_tree(algo, root)
+    og.build_tree(root)
+    val, par, pw = g.labels()
+    np.testing.assert_array_equal(val, og.labels()[0])
+    assert og.validate(val, par, pw, root) == 0
+    if algo == "sswp":
+        assert (pw > (1 << 31)).any()   # some parents are large-weight edges, read back in full
+    np.testing.assert_array_equal(g.get_edge_num(par_e), np.ones(len(par_e), np.uint64))
+    # incremental: insert the rest, then delete the first copies of the parallel pairs and some loaded edges
+    adds = e[imported:]
+    g.apply_add(algo, adds)
+    gone_a = [x for x in adds if og.add_edge(int(x["src"]), int(x["dst"]), int(x["data"])) == 0]
+    og.update_tree_add_batch(*(np.array([x[f] for x in gone_a], np.uint64) for f in ("src", "dst", "data")), root)
+    dels = np.concatenate([e[big][:300][:150], e[:2000]])
+    old = g.apply_del(algo, dels)
+    og_old = np.array([og.del_edge(int(x["src"]), int(x["dst"]), int(x["data"])) for x in dels], np.uint64)
+    np.testing.assert_array_equal(old, og_old)
+    gone = dels[og_old == 1]
+    og.update_tree_del_batch(gone["src"], gone["dst"], gone["data"], root)
+    val, par, pw = g.labels()
+    np.testing.assert_array_equal(val, og.labels()[0])
+    assert og.validate(val, par, pw, root) == 0
+    g.close()
 
 
 @pytest.mark.parametrize("algo", ALGOS)

@@ -88,6 +88,90 @@ def test_static_build_matches_rg_build_tree(algo):
         assert og.validate(vals, pars, pw, root) == 0
 
 
+def static_call(algo, V, E, row, col, w, vals, pars, root=0):
+    P = ctypes.c_void_p
+    return rg.lib().rg_build_tree_csr_static(
+        rg.ALGOS[algo], root, V, E, P(row.data_ptr()), P(col.data_ptr()), P(w.data_ptr()) if w is not None else None,
+        P(vals.data_ptr()), P(pars.data_ptr()), None)
+
+
+@pytest.mark.parametrize("algo", ["sssp", "wcc"])
+def test_static_build_at_the_vertex_limit(algo):
+    """A graph of exactly RG_STATIC_MAX_VERTICES vertices reaches the ends of
+    the label, queue and stamp regions of the static array (WCC starts with
+    every vertex in the queue)."""
+    scale = 20
+    pairs = gen.rmat(scale, n_edges=4 << scale, seed=23)
+    V = 1 << scale
+    assert V == MAX_V
+    root = gen.max_out_degree_vertex(pairs, V)
+    g = gpu_graph(algo, V, pairs)
+    g.build_tree(algo, root)
+    expect = g.values()
+    g.close()
+    row, col, w = csr(pairs, V, algo)
+    vals, _ = run_static(algo, V, row, col, w, root)
+    np.testing.assert_array_equal(vals, expect)
+
+
+def test_static_setup_call_and_no_device_allocation():
+    """The set-up call (vertices == 0, every pointer NULL) succeeds; after a
+    first build, a second build of the same graph leaves the device's free
+    memory unchanged: the call takes nothing beyond its static array."""
+    import torch
+    assert rg.lib().rg_build_tree_csr_static(0, 0, 0, 0, None, None, None, None, None, None) == 0
+    scale = 12
+    pairs = gen.rmat(scale, seed=29)
+    V = 1 << scale
+    row, col, w = csr(pairs, V, "sssp")
+    dev = torch.device("cuda")
+    t_row, t_col, t_w = (torch.from_numpy(x).to(dev) for x in (row, col, w))
+    vals = torch.empty(V, dtype=torch.int64, device=dev)
+    pars = torch.empty(V, dtype=torch.int64, device=dev)
+    assert static_call("sssp", V, len(col), t_row, t_col, t_w, vals, pars) == 0
+    torch.cuda.synchronize()
+    first = vals.clone()
+    free0, _ = torch.cuda.mem_get_info()
+    assert static_call("sssp", V, len(col), t_row, t_col, t_w, vals, pars) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.equal(first, vals)
+
+
+def test_static_rejects_malformed_csr_and_missing_weights():
+    """Each malformed input comes back as a status.  The arrays passed have
+    exactly the sizes declared, and the kernel checks offsets and columns
+    before it reads through them, so nothing is accessed out of range."""
+    import torch
+    dev = torch.device("cuda")
+    V = 4
+    vals = torch.empty(V, dtype=torch.int64, device=dev)
+    pars = torch.empty(V, dtype=torch.int64, device=dev)
+
+    def t(a, dt):
+        return torch.tensor(a, dtype=dt, device=dev)
+
+    # 0 -> 1 -> 2 -> column 7, which is >= V
+    row = t([0, 1, 2, 3, 3], torch.int64)
+    col = t([1, 2, 7], torch.int32)
+    assert static_call("bfs", V, 3, row, col, None, vals, pars) == 2
+    assert b"column" in rg.lib().rg_last_error()
+    # vertex 1's offsets decrease (2 > 1)
+    row = t([0, 2, 1, 3, 3], torch.int64)
+    col = t([1, 2, 3], torch.int32)
+    assert static_call("bfs", V, 3, row, col, None, vals, pars) == 1
+    # SSSP and SSWP without weights
+    row = t([0, 1, 2, 3, 3], torch.int64)
+    for algo in ("sssp", "sswp"):
+        assert static_call(algo, V, 3, row, col, None, vals, pars) == 1
+        assert b"weights" in rg.lib().rg_last_error()
+    # the same well-formed graph still builds afterwards
+    assert static_call("bfs", V, 3, row, col, None, vals, pars) == 0
+    torch.cuda.synchronize()
+    assert vals.cpu().tolist() == [0, 1, 2, 3]
+
+
 def test_static_rejects_graphs_over_the_limit():
     rc = rg.lib().rg_build_tree_csr_static(rg.ALGOS["bfs"], 0, MAX_V + 1, 0, ctypes.c_void_p(8), ctypes.c_void_p(8),
                                            None, ctypes.c_void_p(8), None, None)
