@@ -307,6 +307,7 @@ typedef struct {
   uint32_t instance, type;
   int32_t status;               /* rg_status of the batch that applied it */
   uint32_t epoch_size;
+  uint64_t version;             /* the instance's epochs so far, this one included */
 } rg_completion;
 
 typedef struct {
@@ -375,6 +376,79 @@ typedef struct {
 
 /* Runs the loads of n configs concurrently (one generator thread each). */
 int rg_server_run_load(rg_server *s, const rg_load_config *cfgs, uint64_t n, rg_load_result *results);
+
+/* rg_server_poll that waits up to timeout_us microseconds for a first
+ * completion when none is queued (the network front end's completion thread
+ * uses it instead of polling in a loop). */
+int rg_server_poll_wait(rg_server *s, rg_completion *out, uint64_t cap, uint64_t *n, uint64_t timeout_us);
+
+/* ---- Network front end and write-ahead log --------------------------------
+ * The reference's served driver (src/all_inc_rpc.cpp) takes updates from
+ * remote clients as ClientUpdateRequest structs (core/rpc.hpp:19-32) and
+ * answers each with a ClientUpdateResponse (:34-38); before serving, the first
+ * connection's first requests are clock-synchronisation requests answered with
+ * {0, 0} (src/all_inc_rpc.cpp:277-290, src/rpc_client.cpp:83-90).  With a WAL,
+ * every update is appended to a 4 KB log block and applied only once its block
+ * is durable; the blocks are written one after another (group commit,
+ * src/all_inc_rpc.cpp:306-335,572-589).  The reference moves the structs over
+ * UCX; here they move over TCP, byte for byte in the reference's x86-64
+ * layout below. */
+typedef struct {
+  uint32_t client_id;
+  uint32_t type;              /* 0 add, 1 delete, 2 end (ClientUpdateRequest::Type) */
+  uint64_t src, dst, data;
+  int64_t request_time_ns;    /* the client's std::chrono::high_resolution_clock */
+} rg_client_update_request;   /* 40 bytes (core/rpc.hpp:19-32) */
+
+typedef struct {
+  uint32_t client_id;
+  uint32_t pad;
+  uint64_t version_id;        /* label version after the update (the instance's epoch count) */
+} rg_client_update_response;  /* 16 bytes (core/rpc.hpp:34-38) */
+
+/* One WAL record (the WAL struct of src/all_inc_rpc.cpp:306-316): 32 bytes.
+ * A block is 4096 bytes: uint64 version (1, 2, ...; block k sits at byte
+ * (k - 1) * 4096), uint64 record count, then up to 127 records. */
+typedef struct {
+  uint32_t type;       /* 0 add, 1 delete */
+  uint32_t client_id;
+  uint64_t src, dst, data;
+} rg_wal_record;
+
+typedef struct rg_frontend rg_frontend;
+
+typedef struct {
+  uint64_t connections, requests, updates, sync_requests, wal_blocks, failed;
+  int64_t time_offset_ns;     /* mean (server clock - request_time) of the sync requests */
+  double p50_us, p99_us, p999_us, max_us, mean_us;  /* request_time + offset -> response sent */
+} rg_frontend_stats;
+
+/* Serve `instance` of server s on a TCP listener at host:port (port 0 picks a
+ * free port; rg_frontend_port reports it).  wal_path (nullable) enables the
+ * write-ahead log, truncated at start.  sync_requests: how many clock-sync
+ * requests open the first connection (the reference's clients send 1024;
+ * 0 = none).  The front end drains the server's completion queue, so s should
+ * be a server nothing else polls.  Each connection may carry many clients;
+ * responses on a connection leave in request order.  A request the server
+ * would refuse (vertex id or weight out of range) is answered at once with
+ * version_id ~0 and is neither logged nor applied. */
+int rg_frontend_start(rg_server *s, uint32_t instance, const char *host, uint16_t port, const char *wal_path,
+                      uint32_t sync_requests, rg_frontend **out);
+int rg_frontend_port(rg_frontend *f, uint16_t *port);
+int rg_frontend_stats_get(rg_frontend *f, rg_frontend_stats *st);
+/* Stops accepting, stops reading the connections, waits (up to timeout_ms:
+ * RG_ETIMEOUT) for the updates already taken to complete and be answered,
+ * flushes the WAL and frees the front end. */
+int rg_frontend_stop(rg_frontend *f, uint64_t timeout_ms);
+
+/* Read the records of a WAL file in order (blocks 1, 2, ... until a block is
+ * missing, empty or out of sequence); n = records found (all of them, even
+ * beyond cap).  No GPU needed. */
+int rg_wal_read(const char *path, rg_wal_record *out, uint64_t cap, uint64_t *n);
+/* Re-apply a WAL to a graph whose labels are built for `algo`: the records
+ * in order, runs of adds and runs of deletes as batches (rg_apply_add /
+ * rg_apply_del), which gives the graph and values of the logged run. */
+int rg_wal_replay(rg_graph *g, int algo, const char *path, int directed, uint64_t *applied);
 
 const char *rg_status_string(int status);
 /* Last error message of the calling thread ("" if none). */

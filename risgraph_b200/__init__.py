@@ -16,8 +16,9 @@ import re
 
 import numpy as np
 
-__all__ = ["Graph", "Server", "RGError", "EDGE_DTYPE", "REQUEST_DTYPE", "COMPLETION_DTYPE", "ALGOS", "lib", "gen",
-           "LIB_PATH"]
+__all__ = ["Graph", "Server", "Frontend", "RGError", "EDGE_DTYPE", "REQUEST_DTYPE", "COMPLETION_DTYPE",
+           "CLIENT_REQUEST_DTYPE", "CLIENT_RESPONSE_DTYPE", "WAL_RECORD_DTYPE", "ALGOS", "lib", "gen", "wal_read",
+           "wal_replay", "LIB_PATH"]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "librisgraph_b200.so")
@@ -28,7 +29,13 @@ EDGE_DTYPE = np.dtype([("src", "<u8"), ("dst", "<u8"), ("data", "<u8")])  # rg_e
 REQUEST_DTYPE = np.dtype([("instance", "<u4"), ("type", "<u4"), ("src", "<u8"), ("dst", "<u8"), ("data", "<u8"),
                           ("tag", "<u8")])  # rg_request
 COMPLETION_DTYPE = np.dtype([("tag", "<u8"), ("submit_ns", "<u8"), ("done_ns", "<u8"), ("instance", "<u4"),
-                             ("type", "<u4"), ("status", "<i4"), ("epoch_size", "<u4")])  # rg_completion
+                             ("type", "<u4"), ("status", "<i4"), ("epoch_size", "<u4"), ("version", "<u8")])  # rg_completion
+# the reference's wire structs (core/rpc.hpp:19-38) and WAL record (src/all_inc_rpc.cpp:306-316)
+CLIENT_REQUEST_DTYPE = np.dtype([("client_id", "<u4"), ("type", "<u4"), ("src", "<u8"), ("dst", "<u8"),
+                                 ("data", "<u8"), ("request_time_ns", "<i8")])  # rg_client_update_request
+CLIENT_RESPONSE_DTYPE = np.dtype([("client_id", "<u4"), ("pad", "<u4"), ("version_id", "<u8")])
+WAL_RECORD_DTYPE = np.dtype([("type", "<u4"), ("client_id", "<u4"), ("src", "<u8"), ("dst", "<u8"),
+                             ("data", "<u8")])  # rg_wal_record
 
 _u64 = ctypes.c_uint64
 _ptr = ctypes.c_void_p
@@ -40,6 +47,13 @@ class ServerStats(ctypes.Structure):  # rg_server_stats
     _fields_ = [("completed", ctypes.c_uint64), ("epochs", ctypes.c_uint64), ("largest_epoch", ctypes.c_uint64),
                 ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("p999_us", ctypes.c_double),
                 ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double)]
+
+
+class FrontendStats(ctypes.Structure):  # rg_frontend_stats
+    _fields_ = [("connections", ctypes.c_uint64), ("requests", ctypes.c_uint64), ("updates", ctypes.c_uint64),
+                ("sync_requests", ctypes.c_uint64), ("wal_blocks", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("time_offset_ns", ctypes.c_int64), ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double),
+                ("p999_us", ctypes.c_double), ("max_us", ctypes.c_double), ("mean_us", ctypes.c_double)]
 
 
 class TuneReport(ctypes.Structure):  # rg_tune_report
@@ -125,6 +139,14 @@ def _declare(L):
         "rg_server_stats_get": [P, P, _int],
         "rg_server_run_load": [P, P, _u64, P],
         "rg_server_destroy": [P],
+        "rg_server_poll_wait": [P, P, _u64, P, _u64],
+        "rg_frontend_start": [P, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint16, ctypes.c_char_p, ctypes.c_uint32,
+                              P],
+        "rg_frontend_port": [P, P],
+        "rg_frontend_stats_get": [P, P],
+        "rg_frontend_stop": [P, _u64],
+        "rg_wal_read": [ctypes.c_char_p, P, _u64, P],
+        "rg_wal_replay": [P, _int, ctypes.c_char_p, _int, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -552,3 +574,55 @@ class Server:
         res = (LoadResult * len(loads))()
         _check(lib().rg_server_run_load(self._h, cfgs, len(loads), res), "rg_server_run_load")
         return [_struct_dict(r) for r in res]
+
+
+class Frontend:
+    """Network front end (rg_frontend_*): the reference's ClientUpdateRequest /
+    ClientUpdateResponse structs (core/rpc.hpp:19-38) over TCP into one
+    instance of a Server, with an optional write-ahead log (group commit,
+    src/all_inc_rpc.cpp:306-335).  The server should be one that nothing else
+    polls: the front end drains its completions."""
+
+    def __init__(self, server: "Server", instance: int, host: str = "127.0.0.1", port: int = 0,
+                 wal_path: str | None = None, sync_requests: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().rg_frontend_start(server._h, int(instance), host.encode(), int(port),
+                                       wal_path.encode() if wal_path else None, int(sync_requests), ctypes.byref(h)),
+               "rg_frontend_start")
+        self._h = h
+        p = ctypes.c_uint16()
+        _check(lib().rg_frontend_port(self._h, ctypes.byref(p)), "rg_frontend_port")
+        self.port = p.value
+
+    def stats(self) -> dict:
+        st = FrontendStats()
+        _check(lib().rg_frontend_stats_get(self._h, ctypes.byref(st)), "rg_frontend_stats_get")
+        return _struct_dict(st)
+
+    def stop(self, timeout_ms: int = 60000):
+        if getattr(self, "_h", None):
+            h, self._h = self._h, None
+            _check(lib().rg_frontend_stop(h, int(timeout_ms)), "rg_frontend_stop")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.stop()
+
+
+def wal_read(path: str) -> np.ndarray:
+    """The records of a WAL file, in log order (WAL_RECORD_DTYPE)."""
+    n = _u64()
+    _check(lib().rg_wal_read(path.encode(), None, 0, ctypes.byref(n)), "rg_wal_read")
+    out = np.zeros(n.value, WAL_RECORD_DTYPE)
+    _check(lib().rg_wal_read(path.encode(), _p(out), n.value, ctypes.byref(n)), "rg_wal_read")
+    return out
+
+
+def wal_replay(graph: Graph, algo: str, path: str, directed: bool = True) -> int:
+    """Re-apply a WAL to a graph whose labels are built for algo; returns the records applied."""
+    n = _u64()
+    _check(lib().rg_wal_replay(graph._h, ALGOS[algo], path.encode(), int(directed), ctypes.byref(n)),
+           "rg_wal_replay")
+    return n.value

@@ -33,6 +33,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ccbin", HOST_CXX, "-Xcompi
 
 CU_SOURCES = ["rg_api.cu", "rg_storage.cu", "rg_tree.cu", "rg_static.cu", "rg_serve.cu", "rg_history.cu", "rg_autotune.cu"]
 C_SOURCES = ["rg_gen.c"]
+CXX_SOURCES = ["rg_front.cpp"]
 HEADERS = ["rg_internal.cuh", "rg_storage_dev.cuh"]
 
 
@@ -64,6 +65,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         if force or _newer(o, [s] + hdrs):
             _run([NVCC] + NVFLAGS + ["-c", s, "-o", o], verbose)
+        objs.append(o)
+    for src in CXX_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cpp", ".o"))
+        if force or _newer(o, [s] + hdrs):
+            _run([HOST_CXX, "-O2", "-fPIC", "-std=c++17", "-Wall", "-I" + INCLUDE, "-c", s, "-o", o], verbose)
         objs.append(o)
     for src in C_SOURCES:
         s = os.path.join(CSRC, src)

@@ -160,11 +160,11 @@ void worker_main(rg_server *s, Instance *in) {
     } else if (batch.size() >= in->cap && ms < 0.5 * s->target_ms) {
       in->cap = std::min<uint64_t>(s->max_epoch, in->cap + in->cap / 4 + 1);
     }
-    in->epochs.fetch_add(1, std::memory_order_relaxed);
+    const uint64_t version = in->epochs.fetch_add(1, std::memory_order_relaxed) + 1;
     in->applied.fetch_add(batch.size(), std::memory_order_relaxed);
     out.clear();
     for (const Item &it : batch)
-      out.push_back(rg_completion{it.r.tag, it.submit_ns, t1, in->id, it.r.type, rc, (uint32_t)batch.size()});
+      out.push_back(rg_completion{it.r.tag, it.submit_ns, t1, in->id, it.r.type, rc, (uint32_t)batch.size(), version});
     {
       std::lock_guard<std::mutex> lk(s->cmu);
       for (const rg_completion &c : out) s->lat.push_back(c.done_ns - c.submit_ns);
@@ -306,6 +306,19 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
 
 }  // namespace
 
+namespace rg {
+// The checks rg_server_submit makes, for one request (the network front end
+// refuses a bad update before it reaches the log).
+int server_check(rg_server *s, const rg_request &r) {
+  std::shared_ptr<Instance> in = find(s, r.instance);
+  if (!in) {
+    set_error("unknown instance");
+    return RG_EINVAL;
+  }
+  return check_request(*in, r);
+}
+}  // namespace rg
+
 extern "C" {
 
 int rg_server_create(uint64_t hbm_budget_bytes, double target_epoch_ms, uint64_t max_epoch, int per_update,
@@ -435,6 +448,17 @@ int rg_server_submit(rg_server *s, const rg_request *reqs, uint64_t n) {
 int rg_server_poll(rg_server *s, rg_completion *out, uint64_t cap, uint64_t *n) {
   if (!s || !n || (cap && !out)) return RG_EINVAL;
   std::lock_guard<std::mutex> lk(s->cmu);
+  const uint64_t k = std::min<uint64_t>(cap, s->done.size());
+  std::copy(s->done.begin(), s->done.begin() + k, out);
+  s->done.erase(s->done.begin(), s->done.begin() + k);
+  *n = k;
+  return RG_OK;
+}
+
+int rg_server_poll_wait(rg_server *s, rg_completion *out, uint64_t cap, uint64_t *n, uint64_t timeout_us) {
+  if (!s || !n || (cap && !out)) return RG_EINVAL;
+  std::unique_lock<std::mutex> lk(s->cmu);
+  s->ccv.wait_for(lk, std::chrono::microseconds(timeout_us), [&] { return !s->done.empty(); });
   const uint64_t k = std::min<uint64_t>(cap, s->done.size());
   std::copy(s->done.begin(), s->done.begin() + k, out);
   s->done.erase(s->done.begin(), s->done.begin() + k);

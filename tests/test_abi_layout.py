@@ -17,8 +17,10 @@ HEADER = os.path.join(INCLUDE, "risgraph_b200.h")
 
 # C struct -> its ctypes mirror; C record -> its numpy dtype
 STRUCTS = {"rg_tune_report": rg.TuneReport, "rg_server_stats": rg.ServerStats, "rg_load_config": rg.LoadConfig,
-           "rg_load_result": rg.LoadResult}
-DTYPES = {"rg_edge": rg.EDGE_DTYPE, "rg_request": rg.REQUEST_DTYPE, "rg_completion": rg.COMPLETION_DTYPE}
+           "rg_load_result": rg.LoadResult, "rg_frontend_stats": rg.FrontendStats}
+DTYPES = {"rg_edge": rg.EDGE_DTYPE, "rg_request": rg.REQUEST_DTYPE, "rg_completion": rg.COMPLETION_DTYPE,
+          "rg_client_update_request": rg.CLIENT_REQUEST_DTYPE, "rg_client_update_response": rg.CLIENT_RESPONSE_DTYPE,
+          "rg_wal_record": rg.WAL_RECORD_DTYPE}
 
 
 def _mirror(name):
