@@ -95,17 +95,20 @@ def workload(args):
             "l2": "inputs larger than L2 (edge pool > 126 MB); no flush"}
 
 
-def reached_edges(pairs, V, values, algo):
-    """Distinct stored edges out of reached vertices (both directions for WCC)."""
-    src = pairs[:, 0].astype(np.int64)
-    dst = pairs[:, 1].astype(np.int64)
+def distinct_keys(pairs, V):
+    """Sorted distinct src * V + dst keys of the edge list."""
+    return np.unique(pairs[:, 0].astype(np.int64) * V + pairs[:, 1].astype(np.int64))
+
+
+def reached_edges(pairs, V, values, algo, keys=None):
+    """Distinct stored edges out of reached vertices (both directions for WCC).
+    keys: distinct_keys(pairs, V) when already known."""
+    key = distinct_keys(pairs, V) if keys is None else keys
     if algo == "wcc":
-        key = np.unique(np.concatenate([src * V + dst, dst * V + src]))
-        return int(len(key)), V
+        both = np.unique(np.concatenate([key, (key % V) * V + key // V]))
+        return int(len(both)), V
     reached = values != UNREACHED[algo]
-    key = np.unique(src * V + dst)
-    ks = key // V
-    return int(reached[ks].sum()), int(reached.sum())
+    return int(reached[key // V].sum()), int(reached.sum())
 
 
 def algorithmic_bytes(V, V_r, E_r, algo):
@@ -236,7 +239,7 @@ def timed_builds(g, algo, root, steps, stream):
     return [a.elapsed_time(b) for a, b in ev]
 
 
-def leg_builds(args, peak):
+def leg_builds(args, peak, keys=None):
     """The other algorithms of the full-graph configuration: BFS, SSWP and WCC
     (WCC undirected) builds on RMAT-22, each timed on the device and compared
     with the reference's build of the same graph."""
@@ -248,6 +251,8 @@ def leg_builds(args, peak):
     pairs = gen.rmat(scale, seed=args.seed)
     V = 1 << scale
     root = gen.max_out_degree_vertex(pairs, V)
+    if keys is None:
+        keys = distinct_keys(pairs, V)
     out = {}
     for algo in ("bfs", "sswp", "wcc"):
         directed = algo != "wcc"
@@ -260,10 +265,8 @@ def leg_builds(args, peak):
         values = g.values()
         ms = float(np.mean(timed_builds(g, algo, root, 20, stream)))
         g.close()
-        E_r, V_r = reached_edges(pairs, V, values, algo)
-        alg = algorithmic_bytes(V, V_r, E_r, algo)
-        r = {"gteps": E_r / ms / 1e6, "ms_per_build": ms, "E_r": E_r, "V_r": V_r,
-             "roofline_frac": alg / (ms / 1e3) / 1e9 / peak}
+        r = {"ms_per_build": ms}
+        ref_er = None
         if not args.no_cpu_baseline:
             res, err = ref_driver("build", algo, f"rmat:{scale}:{args.seed}", V, root, 1, 0, timeout=args.ref_timeout)
             if res is None:
@@ -271,8 +274,15 @@ def leg_builds(args, peak):
             else:
                 info, arr = res
                 t = float(np.mean(info["build_times"]))
+                ref_er = info["E_r"]
                 r["values_match_reference"] = bool(np.array_equal(arr["val"], values))
                 r["reference"] = {"gteps": info["E_r"] / t / 1e9, "cores": info["threads"], "E_r": info["E_r"]}
+        if algo == "wcc" and ref_er is not None:
+            E_r, V_r = ref_er, V   # (the both-direction count over the reference's own adjacency)
+        else:
+            E_r, V_r = reached_edges(pairs, V, values, algo, keys)
+        alg = algorithmic_bytes(V, V_r, E_r, algo)
+        r.update({"gteps": E_r / ms / 1e6, "E_r": E_r, "V_r": V_r, "roofline_frac": alg / (ms / 1e3) / 1e9 / peak})
         out[algo] = r
     return out
 
@@ -494,10 +504,11 @@ def leg_served_mix(args):
                        f"{args.mix_think_us:g} us per client, {args.served_seconds:g} s per point",
            "device_bytes": dev}
 
-    def point(srv, ids, total):
+    def point(srv, ids, total, seconds=None):
         per = max(1, total // len(insts))
         loads = [dict(instance=k, clients=per, pairs=i["pairs"], imported=i["imported"],
-                      duration_s=args.served_seconds, think_us=args.mix_think_us, weighted=i["algo"] == "sssp",
+                      duration_s=seconds or args.served_seconds, think_us=args.mix_think_us,
+                      weighted=i["algo"] == "sssp",
                       offset=i["offset"], seed=total, open_loop=1) for k, i in zip(ids, insts)]
         res = srv.run_load(loads)
         st = srv.stats(reset=True)
@@ -514,6 +525,7 @@ def leg_served_mix(args):
         with rg.Server(hbm_budget_bytes=int(dev * 1.05), per_update=per_update, max_epoch=1 << 16,
                        target_epoch_ms=0.4) as srv:
             ids = [srv.attach(i["g"], directed=i["algo"] != "wcc") for i in insts]
+            point(srv, ids, 64, 0.3)   # warm-up, not reported: the first epochs build their cached graphs
             total = 64
             while total <= 16384:
                 pt = point(srv, ids, total)
@@ -714,7 +726,8 @@ def main():
     for _ in range(max(args.warmup, 1)):
         g.build_tree(algo, root)
     values = g.values()
-    E_r, V_r = reached_edges(pairs, V, values, algo)
+    keys = distinct_keys(pairs, V)
+    E_r, V_r = reached_edges(pairs, V, values, algo, keys)
 
     # timed region: device time with CUDA events on the launching stream
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -810,7 +823,8 @@ def main():
     legs = {}
     want = [] if args.legs == "none" else [x for x in args.legs.split(",") if x]
     if rank == 0 and world == 1:
-        fns = {"builds": lambda: leg_builds(args, peak), "bfs_inc": lambda: leg_bfs_inc(args),
+        fns = {"builds": lambda: leg_builds(args, peak, keys),
+               "bfs_inc": lambda: leg_bfs_inc(args),
                "batches": lambda: leg_batches(args), "served": lambda: leg_served(args),
                "served_mix": lambda: leg_served_mix(args), "wcc_del": lambda: leg_wcc_del(args)}
         for name in want:

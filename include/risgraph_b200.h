@@ -206,7 +206,11 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
  *                         (0, the default: 4 |V| + 1024).  A call that reaches
  *                         it stops with RG_ETIMEOUT and leaves the labels
  *                         partly updated; the graph stays usable and the next
- *                         rg_build_tree restores them. */
+ *                         rg_build_tree restores them.
+ *   RG_OPT_PULL_GROUPS    launches of a split pull level (2..16, default 2): the
+ *                         hub slices first, then the other rows, widest first, in
+ *                         groups - 1 launches of about equal entries; each launch
+ *                         reads the values the earlier ones set in this level. */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -217,7 +221,8 @@ typedef enum {
   RG_OPT_PULL_DIV = 6,
   RG_OPT_TINY_EDGES = 7,
   RG_OPT_PULL_SPLIT = 8,
-  RG_OPT_MAX_LEVELS = 9
+  RG_OPT_MAX_LEVELS = 9,
+  RG_OPT_PULL_GROUPS = 10
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

@@ -569,6 +569,10 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
       g.pull_split = (int)value;
       return RG_OK;
     case RG_OPT_MAX_LEVELS: g.max_levels = value; return RG_OK;
+    case RG_OPT_PULL_GROUPS:
+      if (value < 2 || value > 16) break;
+      g.pull_groups = value;
+      return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -588,6 +592,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_TINY_EDGES: *value = g.tiny_edges; return RG_OK;
     case RG_OPT_PULL_SPLIT: *value = (uint64_t)g.pull_split; return RG_OK;
     case RG_OPT_MAX_LEVELS: *value = g.max_levels; return RG_OK;
+    case RG_OPT_PULL_GROUPS: *value = g.pull_groups; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

@@ -291,6 +291,8 @@ struct Graph {
   uint64_t sell_hubs = 0, sell_rows = 0, sell_slices = 0, sell_epoch = 0;
   uint64_t sell_cls[3] = {0, 0, 0};  // first slice of width <= 8, 4, 2
   uint64_t sell_split = 0;           // first slice of the second launch of a pull level
+  std::vector<uint64_t> sell_off_host;  // host copy of sell_off (launch bounds of grouped pull levels)
+  uint64_t pull_groups = 2;          // launches of a split pull level (RG_OPT_PULL_GROUPS)
   uint64_t pull_div = 64;
   int pull_split = 2;  // two-launch pull levels: 1 always, 0 never, 2 SSSP and WCC
   // versioned label history (off until rg_history_enable)

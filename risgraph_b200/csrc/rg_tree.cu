@@ -1123,6 +1123,7 @@ struct LevelCfg {
   uint64_t pull_split;  // pull levels run in two launches
   uint64_t tiny_edges;
   uint64_t max_levels;  // level bound baked into the loop graphs
+  uint64_t pull_groups;  // launches of a split pull level
   int allow_pull;
   int bottom_up;
 };
@@ -1167,7 +1168,7 @@ __global__ void __launch_bounds__(LVB_TPB) k_level_begin(DevGraph g, const uint3
   else if (n >= cfg.lbs_min) mode = M_LBS;
   if (mode == M_DENSE_PUSH) c[C_ACT] += 1;
   c[C_MODE] = mode;
-  if (use_switch) c[C_KLAUNCH] += 1 + mode_launches(mode);
+  if (use_switch) c[C_KLAUNCH] += 1 + mode_launches(mode) + (mode == M_PULL ? cfg.pull_groups - 2 : 0);
   if (n) {
     if (lvl < TRACE_CAP) g.trace[lvl] = n;
     c[C_LEVEL] = lvl + 1;
@@ -1890,6 +1891,9 @@ int prepare_pull_w(Graph &g) {
   g.sell_cls[1] = std::min<uint64_t>(cls[1], g.sell_cls[2]);
   g.sell_cls[0] = std::min<uint64_t>(cls[0], g.sell_cls[1]);
   g.sell_split = std::min<uint64_t>(cls[3], g.sell_cls[0]);
+  g.sell_off_host.resize(slices + 1);
+  RG_CUDA(cudaMemcpyAsync(g.sell_off_host.data(), g.sell_off, (slices + 1) * 8, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
   g.sell_epoch++;
   g.pull_version = g.adj_version;
   return RG_OK;
@@ -1907,6 +1911,27 @@ bool pull_split_on(const Graph &g, int A) {
 int prepare_pull(Graph &g) {
   if (g.pull_version == g.adj_version) return RG_OK;
   return g.weighted ? prepare_pull_w<true>(g) : prepare_pull_w<false>(g);
+}
+
+// Slice bounds of the launches that follow the hub launch of a split pull
+// level: [mid, b1), [b1, b2), ..., [b_k, c8), the narrow classes with the last
+// launch; groups - 1 launches holding about equal shares of the entries of
+// slices [mid, end).
+std::vector<uint64_t> pull_group_bounds(const Graph &g, uint64_t mid, uint64_t c8, uint64_t groups) {
+  std::vector<uint64_t> b{mid};
+  const uint64_t k = groups > 2 ? groups - 1 : 1;
+  const std::vector<uint64_t> &off = g.sell_off_host;
+  if (k > 1 && off.size() == g.sell_slices + 1 && mid <= c8 && c8 <= g.sell_slices) {
+    const uint64_t e0 = off[mid], e1 = off[g.sell_slices];
+    for (uint64_t i = 1; i < k; i++) {
+      const uint64_t target = e0 + (e1 - e0) * i / k;
+      uint64_t s = (uint64_t)(std::lower_bound(off.begin() + mid, off.begin() + c8, target) - off.begin());
+      s = std::min(std::max(s, b.back()), c8);
+      if (s > b.back() && s < c8) b.push_back(s);
+    }
+  }
+  b.push_back(c8);
+  return b;
 }
 
 uint64_t max_levels_of(const Graph &g) { return g.max_levels ? g.max_levels : 4 * (uint64_t)g.V + 1024; }
@@ -1935,9 +1960,14 @@ int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
                                                          mst);
       k_pull_hub_fix<A><<<(unsigned)std::max<uint64_t>(1, (g.sell_hubs + 255) / 256), 256, 0, s>>>(
           g.d, g.sell_hub, g.sell_hub_off, g.sell_hubs, g.sell_piece_best, fout, fout_n, mst);
-      k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(g.d, ent, g.sell_off, g.sell_row, g.sell_rows, g.sell_slices,
-                                                         cls, mid, cls.c8, split ? 1 : 0, g.sell_piece_best, fout,
-                                                         fout_n, mst);
+      // the other rows, in widest-first groups of equal entries: each group
+      // reads the values the groups before it set in this level
+      const std::vector<uint64_t> b = pull_group_bounds(g, mid, cls.c8, split ? g.pull_groups : 2);
+      for (size_t i = 0; i + 1 < b.size(); i++)
+        k_pull_sell<A, W><<<g.num_sms * 8, PS_TPB, 0, s>>>(g.d, ent, g.sell_off, g.sell_row, g.sell_rows,
+                                                           g.sell_slices, cls, b[i], b[i + 1],
+                                                           (split && i + 2 == b.size()) ? 1 : 0, g.sell_piece_best,
+                                                           fout, fout_n, mst);
       break;
     }
     case M_DENSE_PUSH:
@@ -1973,6 +2003,7 @@ uint64_t cfg_key(const LevelCfg &c) {
   h = splitmix64(h ^ c.pull_split);
   h = splitmix64(h ^ c.tiny_edges);
   h = splitmix64(h ^ c.max_levels);
+  h = splitmix64(h ^ c.pull_groups);
   return splitmix64(h ^ ((uint64_t)c.allow_pull << 1) ^ (uint64_t)c.bottom_up);
 }
 
@@ -1987,6 +2018,7 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   cfg.pull_split = pull_split_on(g, A) ? 1 : 0;
   cfg.tiny_edges = g.tiny_edges < TINY_EDGES ? g.tiny_edges : TINY_EDGES;
   cfg.max_levels = max_levels_of(g);
+  cfg.pull_groups = cfg.pull_split ? std::max<uint64_t>(2, g.pull_groups) : 2;
   return cfg;
 }
 
