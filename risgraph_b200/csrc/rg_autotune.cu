@@ -137,7 +137,6 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
     if ((rc = t.tune(RG_OPT_PULL_DIV, {16, 32, 64, 128, 256}, &Tuner::build_ms, &ms))) return rc;
   }
   if (algo != RG_BFS && (rc = t.tune(RG_OPT_PULL_SPLIT, {0, 1}, &Tuner::build_ms, &ms))) return rc;
-  if (algo != RG_BFS && (rc = t.tune(RG_OPT_PULL_GROUPS, {2, 3, 4, 6}, &Tuner::build_ms, &ms))) return rc;
   if ((rc = t.tune(RG_OPT_DENSE_DIV, {10, 20, 40, 80}, &Tuner::build_ms, &ms))) return rc;
   if ((rc = t.tune(RG_OPT_LBS_MIN, {512, 2048, 8192, 32768}, &Tuner::build_ms, &ms))) return rc;
   // small-frontier knob: builds and the sample's round trips together

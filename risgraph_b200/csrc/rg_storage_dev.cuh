@@ -166,6 +166,51 @@ __device__ __forceinline__ void grow_vertex(DevDir dir, unsigned long long *ctl,
   __syncthreads();
 }
 
+// The same growth done by one warp, so that the warps of one CTA grow
+// different vertices at once (the grow list names each vertex once).
+template <bool W>
+__device__ __forceinline__ void grow_vertex_warp(DevDir dir, unsigned long long *ctl, uint32_t v, int lane) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *pool = reinterpret_cast<E *>(dir.pool);
+  unsigned long long new_off = 0;
+  uint32_t new_cap = 0, copy = 0;
+  if (lane == 0) {
+    uint32_t len = dir.len[v], cap = dir.cap[v];
+    if (len > cap) {  // (a retry after compaction skips vertices already grown)
+      uint64_t want = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
+      while (want < len) want *= 2;
+      if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
+      unsigned long long off = atomicAdd(dir.pool_top, (unsigned long long)want);
+      if (off + want > dir.pool_cap) {
+        atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
+        ctl[C_AUX] = 1;
+      } else {
+        new_cap = (uint32_t)want;
+        new_off = off;
+      }
+    }
+    copy = len < cap ? len : cap;
+  }
+  new_cap = __shfl_sync(0xFFFFFFFFu, new_cap, 0);
+  new_off = __shfl_sync(0xFFFFFFFFu, new_off, 0);
+  copy = __shfl_sync(0xFFFFFFFFu, copy, 0);
+  if (new_cap) {
+    const uint64_t from = dir.off[v];
+    const uint32_t old_cap = dir.cap[v];
+    for (uint32_t i = lane; i < copy; i += 32) {
+      pool[new_off + i] = pool[from + i];
+      dir.owner[new_off + i] = v;
+    }
+    for (uint32_t i = lane; i < old_cap; i += 32) dir.owner[from + i] = NONE;
+    __syncwarp();
+    if (lane == 0) {
+      dir.off[v] = new_off;
+      dir.cap[v] = new_cap;
+    }
+  }
+  __syncwarp();
+}
+
 // Store op j's new entries (created by lookup), still DEAD (multiplicity 0).
 template <bool W>
 __device__ __forceinline__ void write_new_op(const DevGraph &g, OpView ops, uint64_t j) {

@@ -1330,7 +1330,6 @@ __global__ void __launch_bounds__(FS_TPB)
     k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data_base, uint64_t *old_host,
                   uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
                   cudaGraphConditionalHandle repair) {
-  __shared__ sdev::GrowShared gsh;
   __shared__ uint64_t s_n, s_pairs, s_want, s_off;
   __shared__ int s_skip;
   unsigned long long *c = g.ctl;
@@ -1379,11 +1378,13 @@ __global__ void __launch_bounds__(FS_TPB)
   for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::lookup_op(g, ops, j, add);
   __syncthreads();
   if (add) {
+    // each warp grows its own vertices (a vertex is in a grow list once)
+    const unsigned gw = tid >> 5, gl = tid & 31;
     const unsigned long long no = c[C_GROWN_OUT];
-    for (unsigned long long k = 0; k < no; k++) sdev::grow_vertex<W>(g.out, c, g.out.grow[k], gsh);
+    for (unsigned long long k = gw; k < no; k += FS_TPB / 32) sdev::grow_vertex_warp<W>(g.out, c, g.out.grow[k], gl);
     if (!g.symmetric) {
       const unsigned long long ni = c[C_GROWN_IN];
-      for (unsigned long long k = 0; k < ni; k++) sdev::grow_vertex<W>(g.in, c, g.in.grow[k], gsh);
+      for (unsigned long long k = gw; k < ni; k += FS_TPB / 32) sdev::grow_vertex_warp<W>(g.in, c, g.in.grow[k], gl);
     }
   }
   __syncthreads();
