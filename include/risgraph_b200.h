@@ -210,7 +210,11 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
  *   RG_OPT_PULL_GROUPS    launches of a split pull level (2..16, default 2): the
  *                         hub slices first, then the other rows, widest first, in
  *                         groups - 1 launches of about equal entries; each launch
- *                         reads the values the earlier ones set in this level. */
+ *                         reads the values the earlier ones set in this level.
+ *   RG_OPT_FUSED_MAX      update batches of at most this many edges (0..2048)
+ *                         take the fused single-CTA path of rg_apply_*: storage
+ *                         and small repairs in one submission; larger batches
+ *                         run grid-wide kernels. */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -222,7 +226,8 @@ typedef enum {
   RG_OPT_TINY_EDGES = 7,
   RG_OPT_PULL_SPLIT = 8,
   RG_OPT_MAX_LEVELS = 9,
-  RG_OPT_PULL_GROUPS = 10
+  RG_OPT_PULL_GROUPS = 10,
+  RG_OPT_FUSED_MAX = 11
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

@@ -457,7 +457,7 @@ class Graph:
 
     OPTIONS = {"dense_pull": 0, "dense_div": 1, "lbs_min": 2, "bfs_bottom_up": 3, "recompute_min": 4, "bu_div": 5,
                "pull_div": 6, "tiny_edges": 7, "pull_split": 8, "max_levels": 9,
-               "pull_groups": 10}
+               "pull_groups": 10, "fused_max": 11}
 
     def set_option(self, name: str, value: int):
         _check(lib().rg_set_option(self._h, self.OPTIONS[name], int(value)), "rg_set_option")

@@ -117,7 +117,7 @@ int edge_updates(rg_graph *gh, const rg_edge *edges, const uint64_t *pairs, uint
   std::vector<rg_edge> wbuf;
   if ((rc = device_edges(g, edges, n, wbuf, &edges))) return rc;
   // small batches (single updates, served epochs): one fused graph launch
-  if (apply && n && n <= rg::SMALL_EDGES && !g.profiling) return rg::apply_small(g, edges, pairs, n, directed, add, old_num);
+  if (apply && n && n <= g.fused_max && !g.profiling) return rg::apply_small(g, edges, pairs, n, directed, add, old_num);
   const int what = add ? 1 : 2;
   for (uint64_t b = 0; b < n; b += CHUNK_EDGES) {
     uint64_t m = std::min(CHUNK_EDGES, n - b), nops = 0;
@@ -237,7 +237,7 @@ int rg_destroy(rg_graph *gh) {
   if (g.stream) cudaStreamSynchronize(g.stream);
   rg::storage_free(g);
   rg::history_free(g);
-  cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
+  cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.chk); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
   cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp); cudaFree(g.act);
   cudaFree(g.sell_ent); cudaFree(g.sell_off); cudaFree(g.sell_row); cudaFree(g.sell_hub); cudaFree(g.sell_piece);
@@ -299,7 +299,7 @@ int rg_apply_add_del(rg_graph *g, int algo, const rg_edge *adds, uint64_t n_add,
   if (!rc) rc = check_edges(g->g, adds, nullptr, n_add);
   if (!rc) rc = check_edges(g->g, dels, nullptr, n_del);
   if (rc) return rc;
-  if (n_add && n_del && n_add <= rg::SMALL_EDGES && n_del <= rg::SMALL_EDGES && !g->g.profiling) {
+  if (n_add && n_del && n_add <= g->g.fused_max && n_del <= g->g.fused_max && !g->g.profiling) {
     std::vector<rg_edge> abuf, dbuf;
     const rg_edge *a = adds, *d = dels;
     if (!rc) rc = device_edges(g->g, adds, n_add, abuf, &a);
@@ -573,6 +573,10 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
       if (value < 2 || value > 16) break;
       g.pull_groups = value;
       return RG_OK;
+    case RG_OPT_FUSED_MAX:
+      if (value > rg::SMALL_EDGES) break;
+      g.fused_max = value;
+      return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -593,6 +597,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_PULL_SPLIT: *value = (uint64_t)g.pull_split; return RG_OK;
     case RG_OPT_MAX_LEVELS: *value = g.max_levels; return RG_OK;
     case RG_OPT_PULL_GROUPS: *value = g.pull_groups; return RG_OK;
+    case RG_OPT_FUSED_MAX: *value = g.fused_max; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

@@ -107,6 +107,7 @@ struct DevGraph {
   uint32_t *val32;   // 32-bit mirror of lab[].x for reads (equal at kernel boundaries)
   uint32_t *stamp;
   uint32_t *inv;
+  uint32_t *chk;     // repair tag of the vertices whose parent chain was found clear in that repair
   uint32_t *modstamp;
   uint32_t *modq;
   unsigned long long *ctl;
@@ -304,6 +305,7 @@ struct Graph {
   int dense_pull = 2;  // dense build levels: 1 = pull over in-edges, 0 = edge-centric push, 2 = pull for WCC only
   uint64_t dense_div = 20, lbs_min = 2048, recompute_min = 2000000;
   uint64_t max_levels = 0;  // bound on the levels of one tree call (0: 4 |V| + 1024)
+  uint64_t fused_max = 2048;  // largest batch of the fused single-CTA apply path (<= SMALL_EDGES)
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]

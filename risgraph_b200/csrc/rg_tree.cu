@@ -1415,19 +1415,34 @@ __global__ void __launch_bounds__(FS_TPB)
 // has_parents (core/graph.hpp:1889-1907): does x's parent chain reach a root
 // without meeting a vertex invalidated (or rescued) by this repair?  The chain
 // guard (0.1 |V| steps) requests a full recompute, as the reference does.
-__device__ __forceinline__ bool has_parents(const DevGraph &g, uint32_t x, uint32_t tag_inv, uint64_t limit) {
+//
+// A chain found clear stays clear for the rest of the repair: tags only go to
+// the tree descendants of vertices tagged before (the seeds are tagged first),
+// and only tagged vertices change parent, so an untagged chain never gains a
+// tag.  The walk therefore stops at a vertex marked clear earlier in this
+// repair (chk == the repair's tag), and a clear walk marks the first vertices
+// of its chain, so that walks from their descendants end there.
+__device__ __forceinline__ bool has_parents(const DevGraph &g, uint32_t x0, uint32_t tag_inv, uint64_t limit) {
   uint64_t num = 0;
+  uint32_t x = x0;
   for (;;) {
+    if (ld_u32(&g.chk[x]) == tag_inv) break;
     uint32_t t = ld_u32(&g.inv[x]);
     if (t == tag_inv || t == tag_inv + 1) return true;
     uint32_t p = (uint32_t)ld_meta(&g.lab[x]);
-    if (p == NONE) return false;
+    if (p == NONE) break;
     x = p;
     if (++num > limit) {
       atomicExch(&g.ctl[C_RECOMPUTE], 1ull);
       return true;
     }
   }
+  x = x0;
+  for (int k = 0; k < 16 && x != NONE && ld_u32(&g.chk[x]) != tag_inv; k++) {
+    g.chk[x] = tag_inv;
+    x = (uint32_t)ld_meta(&g.lab[x]);
+  }
+  return false;
 }
 
 // Rescue (core/graph.hpp:1323-1361): an invalidated dst keeps its value when an
@@ -2372,6 +2387,7 @@ int del_enqueue(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
   if (rc) return rc;
   if (++g.inv_epoch >= 0x7FFFFFFFu) {
     RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+    RG_CUDA(cudaMemsetAsync(g.d.chk, 0, (size_t)g.V * 4, g.stream));
     g.inv_epoch = 1;
   }
   const unsigned long long tag = 2ull * g.inv_epoch;  // tag: invalidated; tag+1: rescued
@@ -2409,6 +2425,7 @@ int after_sync(Graph &g, int what) {
     if (g.h_ctl[C_RECOMPUTE]) {
       g.st_recomputes++;
       RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+      RG_CUDA(cudaMemsetAsync(g.d.chk, 0, (size_t)g.V * 4, g.stream));
       g.inv_epoch = 0;
       int rc = build_enqueue<A, W>(g, g.root);
       if (!rc) rc = read_ctl(g);
@@ -2465,6 +2482,7 @@ int tree_alloc(Graph &g) {
   RG_CUDA(cudaMemset(g.d.val32, 0, V * 4 + 4));
   if ((rc = alloc((void **)&g.d.stamp, V * 4 + 4, "frontier stamps"))) return rc;
   if ((rc = alloc((void **)&g.d.inv, V * 4 + 4, "invalidation tags"))) return rc;
+  if ((rc = alloc((void **)&g.d.chk, V * 4 + 4, "clear-chain marks"))) return rc;
   if ((rc = alloc((void **)&g.d.modstamp, V * 4 + 4, "modified stamps"))) return rc;
   if ((rc = alloc((void **)&g.d.modq, V * 4 + 4, "modified list"))) return rc;
   if ((rc = alloc((void **)&g.q[0], V * 4 + 4, "frontier"))) return rc;
@@ -2491,6 +2509,7 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.d.trace, TRACE_CAP * 8, "level trace"))) return rc;
   RG_CUDA(cudaMemset(g.d.stamp, 0, V * 4 + 4));
   RG_CUDA(cudaMemset(g.d.inv, 0, V * 4 + 4));
+  RG_CUDA(cudaMemset(g.d.chk, 0, V * 4 + 4));
   RG_CUDA(cudaMemset(g.d.modstamp, 0, V * 4 + 4));
   // labels start as "no parent", value 0 until build_tree (alloc_vertex_tree_array, :255-262)
   RG_CUDA(cudaMemset(g.d.lab, 0, V * 16 + 16));
@@ -2693,6 +2712,7 @@ int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_
   if (!add) {
     if (++g.inv_epoch >= 0x7FFFFFFFu) {
       RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+      RG_CUDA(cudaMemsetAsync(g.d.chk, 0, (size_t)g.V * 4, g.stream));
       g.inv_epoch = 1;
     }
     h->inv_tag = 2ull * g.inv_epoch;  // tag: invalidated; tag+1: rescued
@@ -2738,6 +2758,7 @@ int apply_add_del_t(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge
   if ((rc = guard_counters(g))) return rc;
   if (++g.inv_epoch >= 0x7FFFFFFFu) {
     RG_CUDA(cudaMemsetAsync(g.d.inv, 0, (size_t)g.V * 4, g.stream));
+    RG_CUDA(cudaMemsetAsync(g.d.chk, 0, (size_t)g.V * 4, g.stream));
     g.inv_epoch = 1;
   }
   h2->inv_tag = 2ull * g.inv_epoch;

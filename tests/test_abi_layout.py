@@ -79,7 +79,8 @@ def test_option_names_match_header_enum():
     names = {"dense_pull": "DENSE_PULL", "dense_div": "DENSE_DIV", "lbs_min": "LBS_MIN",
              "bfs_bottom_up": "BFS_BOTTOM_UP", "recompute_min": "RECOMPUTE_MIN", "bu_div": "BFS_BU_DIV",
              "pull_div": "PULL_DIV", "tiny_edges": "TINY_EDGES", "pull_split": "PULL_SPLIT",
-             "max_levels": "MAX_LEVELS", "pull_groups": "PULL_GROUPS"}
+             "max_levels": "MAX_LEVELS", "pull_groups": "PULL_GROUPS",
+             "fused_max": "FUSED_MAX"}
     assert set(py) == set(names), set(py) ^ set(names)
     for k, v in py.items():
         assert header[names[k]] == v, k
