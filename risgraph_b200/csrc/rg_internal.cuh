@@ -305,7 +305,9 @@ struct Graph {
   int dense_pull = 2;  // dense build levels: 1 = pull over in-edges, 0 = edge-centric push, 2 = pull for WCC only
   uint64_t dense_div = 20, lbs_min = 2048, recompute_min = 2000000;
   uint64_t max_levels = 0;  // bound on the levels of one tree call (0: 4 |V| + 1024)
-  uint64_t fused_max = 2048;  // largest batch of the fused single-CTA apply path (<= SMALL_EDGES)
+  // largest batch of the fused single-CTA apply path (<= SMALL_EDGES); measured on RMAT-24
+  // SSSP, larger batches run faster on the grid-wide kernels
+  uint64_t fused_max = 1024;
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
