@@ -237,7 +237,7 @@ int rg_destroy(rg_graph *gh) {
   if (g.stream) cudaStreamSynchronize(g.stream);
   rg::storage_free(g);
   rg::history_free(g);
-  cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.chk); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
+  cudaFree(g.d.lab); cudaFree(g.d.val32); cudaFree(g.d.stamp); cudaFree(g.d.inv); cudaFree(g.d.chk); cudaFree(g.d.heavy); cudaFree(g.d.modstamp); cudaFree(g.d.modq);
   cudaFree(g.q[0]); cudaFree(g.q[1]); cudaFree(g.tree); cudaFree(g.scratch64); cudaFree(g.hubq); cudaFree(g.d.ctl);
   cudaFree(g.lb_P); cudaFree(g.lb_tile); cudaFree(g.cub_tmp); cudaFree(g.act);
   cudaFree(g.sell_ent); cudaFree(g.sell_off); cudaFree(g.sell_row); cudaFree(g.sell_hub); cudaFree(g.sell_piece);

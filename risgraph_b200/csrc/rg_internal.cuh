@@ -67,6 +67,9 @@ enum Ctl : int {
   C_INVITER = 24,  // invalidation levels run by the current deletion repair
   C_ROOT = 25,     // root of the label set (init_label_func argument)
   C_HOSTCOND = 26, // a loop condition for the host, when profile mode steps a loop from the host
+  C_HVR = 27,      // heavy vertices queued by the rescue pass of this invalidation level
+  C_HVE = 28,      // ... by the expand pass
+  C_HVP = 29,      // ... by the pull over the reset set
   C_COUNT = 32
 };
 
@@ -108,6 +111,8 @@ struct DevGraph {
   uint32_t *stamp;
   uint32_t *inv;
   uint32_t *chk;     // repair tag of the vertices whose parent chain was found clear in that repair
+  uint32_t *heavy;   // 3 lists of heavy_cap vertices: rescue, expand, pull (deletion repair)
+  uint64_t heavy_cap;
   uint32_t *modstamp;
   uint32_t *modq;
   unsigned long long *ctl;

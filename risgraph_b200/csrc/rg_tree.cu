@@ -1097,6 +1097,9 @@ __device__ __forceinline__ void prologue_ctl(unsigned long long *c, unsigned lon
   c[C_EDGES] = 0;
   c[C_MODE] = M_EMPTY;
   c[C_KLAUNCH] = 0;
+  c[C_HVR] = 0;
+  c[C_HVE] = 0;
+  c[C_HVP] = 0;
   c[C_STAMP] += 1;
 }
 
@@ -1192,7 +1195,9 @@ __global__ void k_inv_begin(DevGraph g, const unsigned long long *fin_n, unsigne
   unsigned long long *c = g.ctl;
   const uint64_t n = *fin_n;
   *fout_n = 0;
-  c[C_KLAUNCH] += 3;  // this kernel, k_rescue, k_expand
+  c[C_HVR] = 0;
+  c[C_HVE] = 0;
+  c[C_KLAUNCH] += 5;  // this kernel, k_rescue, k_rescue_heavy, k_expand, k_expand_heavy
   if (n == 0 || c[C_RECOMPUTE]) return;
   const uint64_t it = c[C_INVITER];
   if (it <= 10 && c[C_TREEN] + n > big) c[C_RECOMPUTE] = 1;
@@ -1213,7 +1218,7 @@ __global__ void k_inv_cond(DevGraph g, const unsigned long long *n_after, uint64
 
 __global__ void k_copy_frontier(DevGraph g, const uint32_t *src, const unsigned long long *src_n, uint32_t *dst,
                                 unsigned long long *dst_n) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) g.ctl[C_KLAUNCH] += 3;  // k_reset, k_pull, this kernel
+  if (blockIdx.x == 0 && threadIdx.x == 0) g.ctl[C_KLAUNCH] += 4;  // k_reset, k_pull, k_pull_heavy, this kernel
   if (g.ctl[C_RECOMPUTE]) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *dst_n = 0;
     return;
@@ -1448,9 +1453,31 @@ __device__ __forceinline__ bool has_parents(const DevGraph &g, uint32_t x0, uint
 // Rescue (core/graph.hpp:1323-1361): an invalidated dst keeps its value when an
 // in-neighbour satisfies equal_func and has a clean parent chain; the parent
 // moves to that in-edge.  One warp per frontier vertex.
+// Heavy vertices: a warp per vertex would scan an RMAT hub's 10^5 edges 32 at
+// a time.  The warp-per-vertex passes of the deletion repair (rescue, expand,
+// the pull over the reset set) queue the vertices whose list is longer than
+// HEAVY_DEG instead, and a second kernel spreads each queued vertex's list over
+// every warp of the grid.  Without a queue (the one-CTA repair, which hands
+// heavy vertices over to the grid-wide one) or when it is full, the warp scans
+// the whole list itself.
+constexpr uint32_t HEAVY_DEG = 2048;
+
+__device__ __forceinline__ bool queue_heavy(uint32_t *hv, unsigned long long *hv_n, uint64_t hv_cap, uint32_t v,
+                                            int lane) {
+  unsigned long long k = 0;
+  if (lane == 0) k = atomicAdd(hv_n, 1ull);
+  k = __shfl_sync(FULL, k, 0);
+  if (k < hv_cap) {
+    if (lane == 0) hv[k] = v;
+    return true;
+  }
+  return false;
+}
+
 template <int A, bool W>
 __device__ __forceinline__ void rescue_warps(const DevGraph &g, const uint32_t *fin, uint64_t n, uint64_t limit,
-                                             uint64_t warp, uint64_t nwarps) {
+                                             uint64_t warp, uint64_t nwarps, uint32_t *hv = nullptr,
+                                             unsigned long long *hv_n = nullptr, uint64_t hv_cap = 0) {
   const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
@@ -1461,6 +1488,7 @@ __device__ __forceinline__ void rescue_warps(const DevGraph &g, const uint32_t *
     const uint64_t sd = ld_v32(g.val32, d);
     const uint32_t len = seg_len(g.in, d);
     const uint64_t off = g.in.off[d];
+    if (hv && len > HEAVY_DEG && queue_heavy(hv, hv_n, hv_cap, d, lane)) continue;
     for (uint32_t kb = 0; kb < len; kb += 32) {
       const uint32_t k = kb + lane;
       bool ok = false;
@@ -1495,7 +1523,46 @@ __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin,
   if (g.ctl[C_RECOMPUTE]) return;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  rescue_warps<A, W>(g, fin, *fin_n, limit, warp, nwarps);
+  rescue_warps<A, W>(g, fin, *fin_n, limit, warp, nwarps, g.heavy, &g.ctl[C_HVR], g.heavy_cap);
+}
+
+// Rescue of the queued heavy vertices: for each in turn, every warp scans a
+// 32-entry stride of its in-list; the first valid candidate wins the CAS.
+template <int A, bool W>
+__global__ void __launch_bounds__(TPB) k_rescue_heavy(DevGraph g, uint64_t limit) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
+  using P = PoolT<W>;
+  const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
+  const int lane = lane_id();
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t nh = min(g.ctl[C_HVR], (unsigned long long)g.heavy_cap);
+  for (uint64_t h = 0; h < nh; h++) {
+    const uint32_t d = g.heavy[h];
+    const uint64_t sd = ld_v32(g.val32, d);
+    const uint32_t len = seg_len(g.in, d);
+    const uint64_t off = g.in.off[d];
+    for (uint64_t kb = warp * 32; kb < len; kb += nwarps * 32) {
+      if (__shfl_sync(FULL, ld_u32(&g.inv[d]), 0) != tag_inv) break;  // rescued by another warp
+      const uint64_t k = kb + lane;
+      bool ok = false;
+      uint32_t src = 0, w = 0;
+      if (k < len) {
+        typename P::E e = pool[off + k];
+        src = P::nbr(e);
+        w = P::wt(e);
+        if (!(src & DEAD) && Hook<A>::combine(ld_v32(g.val32, src), w) == sd) ok = !has_parents(g, src, tag_inv, limit);
+      }
+      unsigned b = __ballot_sync(FULL, ok);
+      if (b) {
+        const int l = __ffs(b) - 1;
+        if (lane == l && atomicCAS(&g.inv[d], tag_inv, tag_inv + 1) == tag_inv)
+          reinterpret_cast<unsigned long long *>(&g.lab[d])[1] = pack_parent(src, w);
+        break;
+      }
+    }
+  }
 }
 
 // Collect and expand (core/graph.hpp:1363-1417): a still-invalid vertex joins
@@ -1503,7 +1570,8 @@ __global__ void __launch_bounds__(TPB) k_rescue(DevGraph g, const uint32_t *fin,
 template <int A, bool W>
 __device__ __forceinline__ void expand_warps(const DevGraph &g, const uint32_t *fin, uint64_t n, uint32_t *tree,
                                              uint32_t *fout, unsigned long long *fout_n, uint64_t warp,
-                                             uint64_t nwarps) {
+                                             uint64_t nwarps, uint32_t *hv = nullptr,
+                                             unsigned long long *hv_n = nullptr, uint64_t hv_cap = 0) {
   const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.out.pool);
@@ -1517,8 +1585,43 @@ __device__ __forceinline__ void expand_warps(const DevGraph &g, const uint32_t *
     }
     const uint32_t len = seg_len(g.out, u);
     const uint64_t off = g.out.off[u];
+    if (hv && len > HEAVY_DEG && queue_heavy(hv, hv_n, hv_cap, u, lane)) continue;
     for (uint32_t kb = 0; kb < len; kb += 32) {
       const uint32_t k = kb + lane;
+      bool app = false;
+      uint32_t v = 0;
+      if (k < len) {
+        typename P::E e = pool[off + k];
+        v = P::nbr(e);
+        if (!(v & DEAD) && ld_meta(&g.lab[v]) == pack_parent(u, P::wt(e))) {
+          uint32_t t = ld_u32(&g.inv[v]);
+          if (t != tag_inv && t != tag_inv + 1) app = atomicCAS(&g.inv[v], t, tag_inv) == t;
+        }
+      }
+      warp_append(app, v, fout, fout_n, FULL);
+    }
+  }
+}
+
+// Expansion of the queued heavy vertices: their tree children, found by every
+// warp over a stride of the out-list.
+template <int A, bool W>
+__global__ void __launch_bounds__(TPB) k_expand_heavy(DevGraph g, uint32_t *fout, unsigned long long *fout_n) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  const uint32_t tag_inv = (uint32_t)g.ctl[C_INVTAG];
+  using P = PoolT<W>;
+  const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.out.pool);
+  const int lane = lane_id();
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t *hv = g.heavy + g.heavy_cap;
+  const uint64_t nh = min(g.ctl[C_HVE], (unsigned long long)g.heavy_cap);
+  for (uint64_t h = 0; h < nh; h++) {
+    const uint32_t u = hv[h];
+    const uint32_t len = seg_len(g.out, u);
+    const uint64_t off = g.out.off[u];
+    for (uint64_t kb = warp * 32; kb < len; kb += nwarps * 32) {
+      const uint64_t k = kb + lane;
       bool app = false;
       uint32_t v = 0;
       if (k < len) {
@@ -1540,7 +1643,8 @@ __global__ void __launch_bounds__(TPB) k_expand(DevGraph g, const uint32_t *fin,
   if (g.ctl[C_RECOMPUTE]) return;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  expand_warps<A, W>(g, fin, *fin_n, tree, fout, fout_n, warp, nwarps);
+  expand_warps<A, W>(g, fin, *fin_n, tree, fout, fout_n, warp, nwarps, g.heavy + g.heavy_cap, &g.ctl[C_HVE],
+                     g.heavy_cap);
 }
 
 // Reset the invalid set to init (core/graph.hpp:1420-1430).
@@ -1572,7 +1676,9 @@ __global__ void k_reset(DevGraph g, const uint32_t *tree, const unsigned long lo
 // vertex takes its best in-neighbour by update_func.  One warp per vertex.
 template <int A, bool W>
 __device__ __forceinline__ unsigned long long pull_warps(const DevGraph &g, const uint32_t *fin, uint64_t n,
-                                                         uint32_t mst, uint64_t warp, uint64_t nwarps) {
+                                                         uint32_t mst, uint64_t warp, uint64_t nwarps,
+                                                         uint32_t *hv = nullptr, unsigned long long *hv_n = nullptr,
+                                                         uint64_t hv_cap = 0) {
   using P = PoolT<W>;
   const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
   const int lane = lane_id();
@@ -1581,6 +1687,7 @@ __device__ __forceinline__ unsigned long long pull_warps(const DevGraph &g, cons
     const uint32_t d = fin[idx];
     const uint32_t len = seg_len(g.in, d);
     const uint64_t off = g.in.off[d];
+    if (hv && len > HEAVY_DEG && queue_heavy(hv, hv_n, hv_cap, d, lane)) continue;
     uint64_t best = ld_v32(g.val32, d), bsu = 0;
     uint32_t bsrc = NONE, bw = 0;
     for (uint32_t k = lane; k < len; k += 32) {
@@ -1613,7 +1720,52 @@ __global__ void __launch_bounds__(TPB) k_pull(DevGraph g, const uint32_t *fin, c
   if (g.ctl[C_RECOMPUTE]) return;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long local = pull_warps<A, W>(g, fin, *fin_n, mst, warp, nwarps);
+  unsigned long long local =
+      pull_warps<A, W>(g, fin, *fin_n, mst, warp, nwarps, g.heavy + 2 * g.heavy_cap, &g.ctl[C_HVP], g.heavy_cap);
+  warp_add_result(local, &g.ctl[C_RESULT]);
+}
+
+// The pull of the queued heavy reset vertices: every warp takes the best of a
+// stride of the in-list and relaxes the vertex with it (the CAS keeps the best).
+template <int A, bool W>
+__global__ void __launch_bounds__(TPB) k_pull_heavy(DevGraph g, uint32_t mst) {
+  if (g.ctl[C_RECOMPUTE]) return;
+  using P = PoolT<W>;
+  const typename P::E *pool = reinterpret_cast<const typename P::E *>(g.in.pool);
+  const int lane = lane_id();
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t *hv = g.heavy + 2 * g.heavy_cap;
+  const uint64_t nh = min(g.ctl[C_HVP], (unsigned long long)g.heavy_cap);
+  unsigned long long local = 0;
+  for (uint64_t h = 0; h < nh; h++) {
+    const uint32_t d = hv[h];
+    const uint32_t len = seg_len(g.in, d);
+    const uint64_t off = g.in.off[d];
+    if (warp * 32 >= len) continue;
+    uint64_t best = ld_v32(g.val32, d), bsu = 0;
+    uint32_t bsrc = NONE, bw = 0;
+    for (uint64_t k = warp * 32 + lane; k < len; k += nwarps * 32) {
+      typename P::E e = pool[off + k];
+      uint32_t s = P::nbr(e);
+      if (s & DEAD) continue;
+      uint64_t su = ld_v32(g.val32, s);
+      uint64_t nv = Hook<A>::combine(su, P::wt(e));
+      if (Hook<A>::better(nv, best)) { best = nv; bsrc = s; bw = P::wt(e); bsu = su; }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      uint64_t ob = __shfl_down_sync(FULL, best, o);
+      uint64_t osu = __shfl_down_sync(FULL, bsu, o);
+      uint32_t os = __shfl_down_sync(FULL, bsrc, o);
+      uint32_t ow = __shfl_down_sync(FULL, bw, o);
+      if (os != NONE && (bsrc == NONE || Hook<A>::better(ob, best))) { best = ob; bsu = osu; bsrc = os; bw = ow; }
+    }
+    bool upd = false;
+    if (lane == 0 && bsrc != NONE) upd = relax<A>(g, bsrc, bsu, d, bw);
+    local += upd;
+    if (mst) mark_modified(g, __shfl_sync(FULL, upd, 0) && lane == 0, d, mst);
+  }
   warp_add_result(local, &g.ctl[C_RESULT]);
 }
 
@@ -1639,12 +1791,27 @@ __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, u
   uint32_t *cur = q0, *nxt = q1;
   unsigned long long *cur_n = &c[C_QN0], *nxt_n = &c[C_QN1];
   for (;;) {
+    // a heavy vertex (a list longer than HEAVY_DEG) in this level's frontier,
+    // or in the reset set once the levels are done, goes to the grid-wide repair
+    int heavy = 0;
+    {
+      const uint64_t n0 = *cur_n;
+      if (n0 && n0 <= DEL_TINY_N) {
+        for (uint64_t i = tid; i < n0; i += DT_TPB)
+          heavy |= seg_len(g.in, cur[i]) > HEAVY_DEG || seg_len(g.out, cur[i]) > HEAVY_DEG;
+      } else if (n0 == 0) {
+        const uint64_t tn = c[C_TREEN];
+        if (tn <= DEL_TINY_TREE)
+          for (uint64_t i = tid; i < tn; i += DT_TPB) heavy |= seg_len(g.in, tree[i]) > HEAVY_DEG;
+      }
+    }
+    heavy = __syncthreads_or(heavy);
     if (tid == 0) {
       const uint64_t n = *cur_n;
       int go = 1;  // 1: run this level; 0: invalidation done; 2: hand over
       if (n == 0 || c[C_RECOMPUTE]) {
         go = 0;
-      } else if (n > DEL_TINY_N) {
+      } else if (n > DEL_TINY_N || heavy) {
         go = 2;
       } else {
         const uint64_t it = c[C_INVITER];
@@ -1658,7 +1825,7 @@ __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, u
           *nxt_n = 0;
         }
       }
-      if (go == 0 && c[C_TREEN] > DEL_TINY_TREE && !c[C_RECOMPUTE]) go = 2;
+      if (go == 0 && (c[C_TREEN] > DEL_TINY_TREE || heavy) && !c[C_RECOMPUTE]) go = 2;
       s_go = go;
     }
     __syncthreads();
@@ -2176,7 +2343,9 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
       unsigned long long *fin_n = &g.d.ctl[C_QN0 + half], *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
       k_inv_begin<<<1, 1, 0, g.cap_stream>>>(g.d, fin_n, fout_n, big);
       k_rescue<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, limit);
+      k_rescue_heavy<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, limit);
       k_expand<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
+      k_expand_heavy<A, W><<<gridw, TPB, 0, g.cap_stream>>>(g.d, g.q[half ^ 1], fout_n);
     }
     k_inv_cond<<<1, 1, 0, g.cap_stream>>>(g.d, &g.d.ctl[C_QN0], (uint64_t)g.V + 2, wh, 1);
     if ((e = cudaStreamEndCapture(g.cap_stream, &body)) != cudaSuccess) break;
@@ -2194,11 +2363,16 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
     if ((e = cudaGraphAddKernelNode(&n1, graph, &wnode, 1, &kp)) != cudaSuccess) break;
     kp.func = (void *)k_pull<A, W>;
     if ((e = cudaGraphAddKernelNode(&n2, graph, &n1, 1, &kp)) != cudaSuccess) break;
+    void *ha[] = {(void *)&g.d, (void *)&mst};
+    kp.func = (void *)k_pull_heavy<A, W>;
+    kp.kernelParams = ha;
+    cudaGraphNode_t n2h;
+    if ((e = cudaGraphAddKernelNode(&n2h, graph, &n2, 1, &kp)) != cudaSuccess) break;
     kp.func = (void *)k_copy_frontier;
     kp.gridDim = dim3(g.num_sms * 4);
     kp.kernelParams = ca;
     cudaGraphNode_t n3;
-    e = cudaGraphAddKernelNode(&n3, graph, &n2, 1, &kp);
+    e = cudaGraphAddKernelNode(&n3, graph, &n2h, 1, &kp);
   } while (0);
   if (e != cudaSuccess) return cuda_fail(e, "building the deletion-repair graph");
   return RG_OK;
@@ -2338,10 +2512,12 @@ int del_repair_stepped(Graph &g) {
     }
     for (int half = 0; half < 2; half++) {
       unsigned long long *fin_n = &g.d.ctl[C_QN0 + half], *fout_n = &g.d.ctl[C_QN0 + (half ^ 1)];
-      count_launch(g, 3);
+      count_launch(g, 5);
       k_inv_begin<<<1, 1, 0, g.stream>>>(g.d, fin_n, fout_n, big);
       k_rescue<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.q[half], fin_n, limit);
+      k_rescue_heavy<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, limit);
       k_expand<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.q[half], fin_n, g.tree, g.q[half ^ 1], fout_n);
+      k_expand_heavy<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.q[half ^ 1], fout_n);
     }
     count_launch(g);
     k_inv_cond<<<1, 1, 0, g.stream>>>(g.d, &g.d.ctl[C_QN0], max_iter, cudaGraphConditionalHandle{}, 0);
@@ -2349,9 +2525,10 @@ int del_repair_stepped(Graph &g) {
     if ((rc = read_ctl(g))) return rc;
     if (!g.h_ctl[C_HOSTCOND]) break;
   }
-  count_launch(g, 3);
+  count_launch(g, 4);
   k_reset<A><<<gridw, TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
   k_pull<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], mst);
+  k_pull_heavy<A, W><<<gridw, TPB, 0, g.stream>>>(g.d, mst);
   k_copy_frontier<<<g.num_sms * 4, TPB, 0, g.stream>>>(g.d, g.tree, &g.d.ctl[C_TREEN], g.q[0], &g.d.ctl[C_QN0]);
   RG_CUDA(cudaGetLastError());
   return RG_OK;
@@ -2483,6 +2660,9 @@ int tree_alloc(Graph &g) {
   if ((rc = alloc((void **)&g.d.stamp, V * 4 + 4, "frontier stamps"))) return rc;
   if ((rc = alloc((void **)&g.d.inv, V * 4 + 4, "invalidation tags"))) return rc;
   if ((rc = alloc((void **)&g.d.chk, V * 4 + 4, "clear-chain marks"))) return rc;
+  // at most (edge slots / HEAVY_DEG) vertices have a longer list
+  g.d.heavy_cap = std::max(g.d.out.pool_cap, g.d.in.pool_cap) / HEAVY_DEG + 1024;
+  if ((rc = alloc((void **)&g.d.heavy, 3 * g.d.heavy_cap * 4, "heavy-vertex lists"))) return rc;
   if ((rc = alloc((void **)&g.d.modstamp, V * 4 + 4, "modified stamps"))) return rc;
   if ((rc = alloc((void **)&g.d.modq, V * 4 + 4, "modified list"))) return rc;
   if ((rc = alloc((void **)&g.q[0], V * 4 + 4, "frontier"))) return rc;

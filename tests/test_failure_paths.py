@@ -181,3 +181,41 @@ def test_history_matches_reference_mvvec(algo):
     after = np.concatenate([g.history_get(vids.astype(np.uint64), t)[0] for t in range(T, last + 1)])
     np.testing.assert_array_equal(after, ref[T * len(vids):])
     g.close()
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "sswp", "wcc"])
+def test_deletion_repair_splits_heavy_vertices(algo):
+    """The parent edges of the eight heaviest vertices (in-lists of thousands of
+    entries) are deleted, every copy of each: the one-CTA repair hands the
+    hubs to the grid-wide repair, whose rescue, expansion and pull spread each
+    hub's list over all warps.  Values equal the oracle's after the same batch."""
+    scale = 16
+    pairs = gen.rmat(scale, seed=91)
+    V = 1 << scale
+    directed = algo != "wcc"
+    g = gpu_graph(algo, V, pairs, inc_mode=True)
+    og = oracle_graph(algo, V, pairs, inc_mode=True)
+    root = gen.max_out_degree_vertex(pairs, V)
+    g.build_tree(algo, root)
+    og.build_tree(root)
+    val, par, pw = g.labels()
+    _, indeg = g.degrees()
+    order = np.argsort(-indeg.astype(np.int64))
+    hubs = [int(v) for v in order[:64] if par[v] != V and v != root][:8]
+    assert len(hubs) == 8 and indeg[hubs[0]] > 4 * 2048
+    one = np.zeros(len(hubs), rg.EDGE_DTYPE)
+    one["src"], one["dst"] = par[hubs], hubs
+    if WEIGHTED[algo]:
+        one["data"] = pw[hubs]
+    counts = g.get_edge_num(one)
+    if not directed:   # an undirected edge is stored once per orientation: one delete removes a copy of both
+        counts = np.maximum(counts, 1)
+    dels = np.repeat(one, counts.astype(np.int64))
+    g.apply_del(algo, dels, directed)
+    og_old = np.array([og.del_edge(int(e["src"]), int(e["dst"]), int(e["data"])) for e in dels], np.uint64)
+    gone = dels[og_old == 1]
+    og.update_tree_del_batch(gone["src"], gone["dst"], gone["data"], root)
+    val, par, pw = g.labels()
+    np.testing.assert_array_equal(val, og.labels()[0])
+    assert og.validate(val, par, pw, root) == 0
+    g.close()
