@@ -436,7 +436,7 @@ def leg_served(args):
                     best = pt
                 if r["p99_us"] > 1000.0 and c >= 4:
                     break
-                c *= 2
+                c = c * 2 if c < 1024 else c * 3 // 2   # finer steps where the knee lies
             srv.detach(k)
         out[mode] = {"best_at_p99_le_1ms": best, "sweep": sweep}
     inc = g.values()

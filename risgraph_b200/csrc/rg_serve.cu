@@ -176,9 +176,11 @@ void worker_main(rg_server *s, Instance *in) {
     // Adapt the cap to keep one epoch within the target (cf. the threshold
     // update of src/sssp_inc_rt.cpp:394-412, driven by time instead of timeouts).
     const double ms = (t1 - t0) * 1e-6;
+    // (epochs cost a fixed ~50 us plus a small share per update, so the cap
+    // grows while an epoch stays under 3/4 of the target)
     if (ms > s->target_ms && in->cap > 1) {
       in->cap = std::max<uint64_t>(1, in->cap * 3 / 4);
-    } else if (batch.size() >= in->cap && ms < 0.5 * s->target_ms) {
+    } else if (batch.size() >= in->cap && ms < 0.75 * s->target_ms) {
       in->cap = std::min<uint64_t>(s->max_epoch, in->cap + in->cap / 4 + 1);
     }
     const uint64_t version = in->epochs.fetch_add(1, std::memory_order_relaxed) + 1;

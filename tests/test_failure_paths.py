@@ -202,7 +202,7 @@ def test_deletion_repair_splits_heavy_vertices(algo):
     _, indeg = g.degrees()
     order = np.argsort(-indeg.astype(np.int64))
     hubs = [int(v) for v in order[:64] if par[v] != V and v != root][:8]
-    assert len(hubs) == 8 and indeg[hubs[0]] > 4 * 2048
+    assert len(hubs) == 8 and indeg[hubs[0]] > 2048   # above the split threshold (HEAVY_DEG)
     one = np.zeros(len(hubs), rg.EDGE_DTYPE)
     one["src"], one["dst"] = par[hubs], hubs
     if WEIGHTED[algo]:
