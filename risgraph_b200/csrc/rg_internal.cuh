@@ -70,6 +70,7 @@ enum Ctl : int {
   C_HVR = 27,      // heavy vertices queued by the rescue pass of this invalidation level
   C_HVE = 28,      // ... by the expand pass
   C_HVP = 29,      // ... by the pull over the reset set
+  C_OVER = 30,     // the fused apply's one-CTA deletion repair handed over to the grid-wide one
   C_COUNT = 32
 };
 

@@ -77,13 +77,15 @@ __device__ __forceinline__ void lookup_op(const DevGraph &g, OpView ops, uint64_
     if ((uint32_t)e.x == NONE) {
       if (!create) break;
       if (mine == UNSET) {
+        // (no fence before the claim below: a thread that finds this record
+        // in the index only takes its id; the record's fields are read after
+        // the kernel or CTA barrier that ends the lookup step)
         unsigned long long r = atomicAdd(g.rec_top, 1ull);
         if (r >= g.rec_cap) { set_err(g.ctl, RG_ENOSPACE); break; }
         mine = (uint32_t)r;
         g.rec_num[mine] = 0;
         g.rec_out[mine] = UNSET;
         g.rec_in[mine] = UNSET;
-        __threadfence();
       }
       ulonglong2 want = make_ulonglong2(key.x, key.y | ((uint64_t)mine << 32));
       ulonglong2 old = cas128(&g.ht[h], make_ulonglong2(~0ull, ~0ull), want);
@@ -167,13 +169,18 @@ __device__ __forceinline__ void grow_vertex(DevDir dir, unsigned long long *ctl,
 }
 
 // The same growth done by one warp, so that the warps of one CTA grow
-// different vertices at once (the grow list names each vertex once).
-template <bool W>
-__device__ __forceinline__ void grow_vertex_warp(DevDir dir, unsigned long long *ctl, uint32_t v, int lane) {
-  using E = typename std::conditional<W, uint2, uint32_t>::type;
-  E *pool = reinterpret_cast<E *>(dir.pool);
-  unsigned long long new_off = 0;
-  uint32_t new_cap = 0, copy = 0;
+// different vertices at once (the grow list names each vertex once).  The
+// claim (new region from the bump pointer), the copy and the publication of
+// the new offset and capacity are separate steps, so that a long list can be
+// copied by the whole CTA instead (grow_vertex_warp returns such a claim
+// uncopied when `defer` is set).
+struct GrowClaim {
+  unsigned long long new_off, from;
+  uint32_t new_cap, copy, old_cap, v;
+};
+
+__device__ __forceinline__ GrowClaim grow_claim_warp(DevDir dir, unsigned long long *ctl, uint32_t v, int lane) {
+  GrowClaim cl = {0, 0, 0, 0, 0, v};
   if (lane == 0) {
     uint32_t len = dir.len[v], cap = dir.cap[v];
     if (len > cap) {  // (a retry after compaction skips vertices already grown)
@@ -185,30 +192,70 @@ __device__ __forceinline__ void grow_vertex_warp(DevDir dir, unsigned long long 
         atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
         ctl[C_AUX] = 1;
       } else {
-        new_cap = (uint32_t)want;
-        new_off = off;
+        cl.new_cap = (uint32_t)want;
+        cl.new_off = off;
+        cl.from = dir.off[v];
+        cl.old_cap = cap;
       }
     }
-    copy = len < cap ? len : cap;
+    cl.copy = len < cap ? len : cap;
   }
-  new_cap = __shfl_sync(0xFFFFFFFFu, new_cap, 0);
-  new_off = __shfl_sync(0xFFFFFFFFu, new_off, 0);
-  copy = __shfl_sync(0xFFFFFFFFu, copy, 0);
-  if (new_cap) {
-    const uint64_t from = dir.off[v];
-    const uint32_t old_cap = dir.cap[v];
-    for (uint32_t i = lane; i < copy; i += 32) {
-      pool[new_off + i] = pool[from + i];
-      dir.owner[new_off + i] = v;
+  cl.new_cap = __shfl_sync(0xFFFFFFFFu, cl.new_cap, 0);
+  cl.new_off = __shfl_sync(0xFFFFFFFFu, cl.new_off, 0);
+  cl.from = __shfl_sync(0xFFFFFFFFu, cl.from, 0);
+  cl.copy = __shfl_sync(0xFFFFFFFFu, cl.copy, 0);
+  cl.old_cap = __shfl_sync(0xFFFFFFFFu, cl.old_cap, 0);
+  return cl;
+}
+
+// Copies a claimed vertex's slots (thread t of n threads), four loads in
+// flight per thread before their stores.
+template <bool W>
+__device__ __forceinline__ void grow_copy(DevDir dir, const GrowClaim &cl, uint32_t t, uint32_t n) {
+  using E = typename std::conditional<W, uint2, uint32_t>::type;
+  E *pool = reinterpret_cast<E *>(dir.pool);
+  for (uint32_t b = 0; b < cl.copy; b += 4 * n) {
+    E x[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t i = b + k * n + t;
+      if (i < cl.copy) x[k] = pool[cl.from + i];
     }
-    for (uint32_t i = lane; i < old_cap; i += 32) dir.owner[from + i] = NONE;
-    __syncwarp();
-    if (lane == 0) {
-      dir.off[v] = new_off;
-      dir.cap[v] = new_cap;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t i = b + k * n + t;
+      if (i < cl.copy) {
+        pool[cl.new_off + i] = x[k];
+        dir.owner[cl.new_off + i] = cl.v;
+      }
     }
   }
+  for (uint32_t i = t; i < cl.old_cap; i += n) dir.owner[cl.from + i] = NONE;
+}
+
+__device__ __forceinline__ void grow_publish(DevDir dir, const GrowClaim &cl) {
+  dir.off[cl.v] = cl.new_off;
+  dir.cap[cl.v] = cl.new_cap;
+}
+
+// Returns true when the claim was left uncopied for the caller (`defer` and a
+// copy of more than GROW_WARP_MAX slots).
+constexpr uint32_t GROW_WARP_MAX = 2048;
+
+template <bool W>
+__device__ __forceinline__ bool grow_vertex_warp(DevDir dir, unsigned long long *ctl, uint32_t v, int lane,
+                                                 bool defer = false, GrowClaim *out = nullptr) {
+  const GrowClaim cl = grow_claim_warp(dir, ctl, v, lane);
+  if (!cl.new_cap) return false;
+  if (defer && cl.copy > GROW_WARP_MAX) {
+    *out = cl;
+    return true;
+  }
+  grow_copy<W>(dir, cl, (uint32_t)lane, 32);
   __syncwarp();
+  if (lane == 0) grow_publish(dir, cl);
+  __syncwarp();
+  return false;
 }
 
 // Store op j's new entries (created by lookup), still DEAD (multiplicity 0).

@@ -982,11 +982,17 @@ constexpr uint32_t TINY_N = 1024;
 constexpr uint64_t TINY_EDGES = 1ull << 20;
 constexpr int TINY_TPB = 1024;
 
+//
+// tiny_levels is that loop as a device function for a CTA of TINY_TPB threads:
+// it leaves the frontier in q_final (one of q_in, q_out) with its count in
+// *n_final.  first_begun: k_level_begin did the first level's bookkeeping (the
+// level counter, stamp, depth and trace); otherwise the loop does it for every
+// level, the first included.
 template <int A, bool W>
-__global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_in, unsigned long long *n_in,
-                                                        uint32_t *q_out, unsigned long long *n_out,
-                                                        uint64_t max_levels, uint64_t max_edges, uint32_t mst) {
-  if (g.ctl[C_MODE] != M_TINY) return;
+__device__ __forceinline__ void tiny_levels(const DevGraph &g, uint32_t *q_in, unsigned long long *n_in,
+                                            uint32_t *q_out, unsigned long long *n_out, uint32_t *q_final,
+                                            unsigned long long *n_final, uint64_t max_levels, uint64_t max_edges,
+                                            uint32_t mst, bool first_begun) {
   using P_ = PoolT<W>;
   using Scan = cub::BlockScan<uint32_t, TINY_TPB>;
   __shared__ typename Scan::TempStorage scan_tmp;
@@ -1018,7 +1024,7 @@ __global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_
     if (tid == 0) {
       s_pref[TINY_N] = total;
       bool go = n > 0 && n <= TINY_N && total <= max_edges;
-      if (!first && go) {
+      if ((!first || !first_begun) && go) {
         // a new level: the bookkeeping k_level_begin does for the first one
         const uint64_t lvl = c[C_LEVEL];
         go = lvl < max_levels;
@@ -1064,15 +1070,24 @@ __global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_
     cur_n = nxt_n;
     nxt_n = tn;
   }
-  // leave the frontier in the output queue of the level the launch stands for
-  if (cur != q_out) {
+  if (cur != q_final) {
     const uint64_t n = *cur_n;
-    for (uint64_t i = tid; i < n; i += TINY_TPB) q_out[i] = cur[i];
+    for (uint64_t i = tid; i < n; i += TINY_TPB) q_final[i] = cur[i];
     __syncthreads();
-    if (tid == 0) *n_out = n;
+    if (tid == 0) *n_final = n;
   }
+  __syncthreads();
   warp_add_result(local, &c[C_RESULT]);
   warp_add_result(scanned, &c[C_EDGES]);
+}
+
+// The frontier is left in the output queue of the level the launch stands for.
+template <int A, bool W>
+__global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_in, unsigned long long *n_in,
+                                                        uint32_t *q_out, unsigned long long *n_out,
+                                                        uint64_t max_levels, uint64_t max_edges, uint32_t mst) {
+  if (g.ctl[C_MODE] != M_TINY) return;
+  tiny_levels<A, W>(g, q_in, n_in, q_out, n_out, q_out, n_out, max_levels, max_edges, mst, true);
 }
 
 // ---- device-driven level loop ------------------------------------------------
@@ -1087,6 +1102,7 @@ __global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_
 __device__ __forceinline__ void prologue_ctl(unsigned long long *c, unsigned long long inv_tag) {
   c[C_INVTAG] = inv_tag;
   c[C_INVITER] = 0;
+  c[C_OVER] = 0;
   c[C_QN0] = 0;
   c[C_QN1] = 0;
   c[C_HUBN] = 0;
@@ -1317,104 +1333,6 @@ __global__ void k_seed_del(DevGraph g, const uint32_t *os, const uint32_t *od, c
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   seed_del(g, os, od, ow, cand, n, directed, fout, fout_n, warp, nwarps);
-}
-
-// Fused small-batch apply: one CTA runs the storage steps of a batch of at
-// most SMALL_EDGES edges (unpack from the mapped staging buffer, lookup/create,
-// growth, new-slot write, multiplicity count, candidates) and the seeding of
-// the tree repair, with CTA barriers where the multi-kernel path has kernel
-// boundaries.  It then opens the conditional node that runs the repair loops
-// only when the seeds produced a frontier: a safe update (the common case,
-// need_update_tree_* false) costs this one kernel.  A storage error (edge index
-// or pool full) stops before the count step, leaving the op arrays for the
-// host's compaction and replay, exactly like the multi-kernel path.
-constexpr int FS_TPB = 1024;
-
-template <int A, bool W>
-__global__ void __launch_bounds__(FS_TPB)
-    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data_base, uint64_t *old_host,
-                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
-                  cudaGraphConditionalHandle repair) {
-  __shared__ uint64_t s_n, s_pairs, s_want, s_off;
-  __shared__ int s_skip;
-  unsigned long long *c = g.ctl;
-  const unsigned tid = threadIdx.x;
-  if (tid == 0) {
-    // the second batch of a submission does nothing after an error in the first
-    s_skip = second && c[C_ERR] != 0;
-    if (!s_skip) {
-      // the host wrote the header before the launch; read it past any cache
-      s_n = __ldcv(&hdr->n);
-      s_pairs = __ldcv(&hdr->pairs);
-      s_want = __ldcv(&hdr->want_old);
-      s_off = __ldcv(&hdr->data_off);
-      const unsigned long long kl = c[C_KLAUNCH];
-      prologue_ctl(c, __ldcv(&hdr->inv_tag));
-      if (second) c[C_KLAUNCH] = kl;  // the count covers the whole submission
-      c[C_CANDN] = 0;
-      c[C_GROWN_OUT] = 0;
-      c[C_GROWN_IN] = 0;
-    }
-  }
-  __syncthreads();
-  if (s_skip) {
-    if (tid == 0) cudaGraphSetConditional(repair, 0u);
-    return;
-  }
-  const void *data = data_base + s_off;
-  const uint64_t n = s_n < SMALL_EDGES ? s_n : SMALL_EDGES;
-  const uint64_t nops = directed ? n : 2 * n;
-  const int weighted = W ? 1 : 0;
-  if (s_pairs) {
-    const uint64_t *p = reinterpret_cast<const uint64_t *>(data);
-    for (uint64_t i = tid; i < n; i += FS_TPB) {
-      uint64_t s64 = __ldcv(&p[2 * i]), d64 = __ldcv(&p[2 * i + 1]);
-      uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
-      sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, w, directed);
-    }
-  } else {
-    const uint64_t *e = reinterpret_cast<const uint64_t *>(data);
-    for (uint64_t i = tid; i < n; i += FS_TPB) {
-      uint64_t s64 = __ldcv(&e[3 * i]), d64 = __ldcv(&e[3 * i + 1]), w64 = __ldcv(&e[3 * i + 2]);
-      sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, weighted ? (uint32_t)w64 : 0u, directed);
-    }
-  }
-  __syncthreads();
-  for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::lookup_op(g, ops, j, add);
-  __syncthreads();
-  if (add) {
-    // each warp grows its own vertices (a vertex is in a grow list once)
-    const unsigned gw = tid >> 5, gl = tid & 31;
-    const unsigned long long no = c[C_GROWN_OUT];
-    for (unsigned long long k = gw; k < no; k += FS_TPB / 32) sdev::grow_vertex_warp<W>(g.out, c, g.out.grow[k], gl);
-    if (!g.symmetric) {
-      const unsigned long long ni = c[C_GROWN_IN];
-      for (unsigned long long k = gw; k < ni; k += FS_TPB / 32) sdev::grow_vertex_warp<W>(g.in, c, g.in.grow[k], gl);
-    }
-  }
-  __syncthreads();
-  if (c[C_ERR]) {
-    if (tid == 0) cudaGraphSetConditional(repair, 0u);
-    return;
-  }
-  if (add) {
-    for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::write_new_op<W>(g, ops, j);
-    __syncthreads();
-  }
-  for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::count_op<W>(g, ops, j, add);
-  __syncthreads();
-  for (uint64_t i = tid; i < n; i += FS_TPB) sdev::edge_old(ops, i, directed, add, 1, s_want ? old_host : nullptr, cand, c);
-  __syncthreads();
-  const uint64_t ncand = c[C_CANDN];
-  const uint64_t warp = tid >> 5, nwarps = FS_TPB / 32;
-  if (add) {
-    unsigned long long local = seed_add<A>(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], mst, warp, nwarps);
-    warp_add_result(local, &c[C_RESULT]);
-  } else {
-    seed_del(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], warp, nwarps);
-  }
-  __syncthreads();
-  if (tid == 0) cudaGraphSetConditional(repair, (c[C_QN0] && !c[C_ERR]) ? 1u : 0u);
 }
 
 // has_parents (core/graph.hpp:1889-1907): does x's parent chain reach a root
@@ -1778,12 +1696,11 @@ __global__ void __launch_bounds__(TPB) k_pull_heavy(DevGraph g, uint32_t mst) {
 constexpr int DT_TPB = 1024;
 constexpr uint64_t DEL_TINY_N = 1024, DEL_TINY_TREE = 8192;
 
-// in_graph = 0: launched by the host (profile mode); the hand-over decision
-// goes to C_HOSTCOND instead of the IF node's handle.
+// del_tiny_levels is that repair as a device function for a CTA of DT_TPB
+// threads; it returns true when it hands over.
 template <int A, bool W>
-__global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, uint32_t *q1, uint32_t *tree,
-                                                     uint64_t limit, uint64_t big, uint64_t max_iter, uint32_t mst,
-                                                     cudaGraphConditionalHandle standard, int in_graph) {
+__device__ __forceinline__ bool del_tiny_levels(const DevGraph &g, uint32_t *q0, uint32_t *q1, uint32_t *tree,
+                                                uint64_t limit, uint64_t big, uint64_t max_iter, uint32_t mst) {
   __shared__ int s_go;
   unsigned long long *c = g.ctl;
   const unsigned tid = threadIdx.x;
@@ -1850,12 +1767,8 @@ __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, u
       __syncthreads();
       if (tid == 0) c[C_QN0] = n;
     }
-    if (tid == 0) {
-      c[C_KLAUNCH] += 1;
-      if (in_graph) cudaGraphSetConditional(standard, 1u);
-      else c[C_HOSTCOND] = 1;
-    }
-    return;
+    __syncthreads();
+    return true;
   }
   unsigned long long local = 0;
   const bool recompute = c[C_RECOMPUTE] != 0;
@@ -1872,10 +1785,183 @@ __global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, u
     c[C_QN0] = 0;
   }
   warp_add_result(local, &c[C_RESULT]);
+  __syncthreads();
+  return false;
+}
+
+// in_graph = 0: launched by the host (profile mode); the hand-over decision
+// goes to C_HOSTCOND instead of the IF node's handle.
+template <int A, bool W>
+__global__ void __launch_bounds__(DT_TPB) k_del_tiny(DevGraph g, uint32_t *q0, uint32_t *q1, uint32_t *tree,
+                                                     uint64_t limit, uint64_t big, uint64_t max_iter, uint32_t mst,
+                                                     cudaGraphConditionalHandle standard, int in_graph) {
+  const bool over = del_tiny_levels<A, W>(g, q0, q1, tree, limit, big, max_iter, mst);
+  if (threadIdx.x == 0) {
+    g.ctl[C_KLAUNCH] += 1;
+    if (in_graph) cudaGraphSetConditional(standard, over ? 1u : 0u);
+    else g.ctl[C_HOSTCOND] = over ? 1 : 0;
+  }
+}
+
+// The hand-over decision of the fused apply kernel's deletion repair, for the
+// IF node of the grid-wide repair (a kernel sets the handle of a conditional
+// node in its own graph).
+__global__ void k_handover(DevGraph g, cudaGraphConditionalHandle standard) {
+  g.ctl[C_KLAUNCH] += 1;
+  cudaGraphSetConditional(standard, g.ctl[C_OVER] ? 1u : 0u);
+}
+
+// Fused small-batch apply: one CTA runs the storage steps of a batch of at
+// most SMALL_EDGES edges (unpack from the mapped staging buffer, lookup/create,
+// growth, new-slot write, multiplicity count, candidates) and the seeding of
+// the tree repair, with CTA barriers where the multi-kernel path has kernel
+// boundaries.  A small repair then runs in the same CTA: the one-CTA deletion
+// repair (del_tiny_levels) for a delete batch, and push levels while the
+// frontier stays small (tiny_levels).  Only what is left opens the conditional
+// node after the kernel (`repair`), whose body runs the grid-wide deletion
+// repair when the one-CTA repair handed over (C_OVER) and the level loop.  A
+// safe update (the common case, need_update_tree_* false) and most unsafe
+// single updates cost this one kernel.  A storage error (edge
+// index or pool full) stops before the count step, leaving the op arrays for
+// the host's compaction and replay, exactly like the multi-kernel path.
+constexpr int FS_TPB = 1024;
+static_assert(FS_TPB == TINY_TPB && FS_TPB == DT_TPB, "the fused kernel runs the one-CTA repairs");
+
+// What the fused kernel's in-place repair needs besides queue 0.
+struct FusedRepair {
+  uint32_t *q1, *tree;
+  uint64_t limit;       // has_parents chain guard
+  uint64_t big;         // invalidated-set size that asks for a full recompute
+  uint64_t max_iter;    // invalidation levels
+  uint64_t max_levels;  // level bound of the push loop
+  uint64_t tiny_edges;  // out-slot limit of an in-place push level (0: none in place)
+};
+
+template <int A, bool W>
+__global__ void __launch_bounds__(FS_TPB)
+    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data_base, uint64_t *old_host,
+                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
+                  cudaGraphConditionalHandle repair, FusedRepair fr) {
+  __shared__ uint64_t s_n, s_pairs, s_want, s_off;
+  __shared__ int s_skip;
+  unsigned long long *c = g.ctl;
+  const unsigned tid = threadIdx.x;
   if (tid == 0) {
-    c[C_KLAUNCH] += 1;
-    if (in_graph) cudaGraphSetConditional(standard, 0u);
-    else c[C_HOSTCOND] = 0;
+    // the second batch of a submission does nothing after an error in the first
+    s_skip = second && c[C_ERR] != 0;
+    if (!s_skip) {
+      // the host wrote the header before the launch; read it past any cache
+      s_n = __ldcv(&hdr->n);
+      s_pairs = __ldcv(&hdr->pairs);
+      s_want = __ldcv(&hdr->want_old);
+      s_off = __ldcv(&hdr->data_off);
+      const unsigned long long kl = c[C_KLAUNCH];
+      prologue_ctl(c, __ldcv(&hdr->inv_tag));
+      if (second) c[C_KLAUNCH] = kl;  // the count covers the whole submission
+      c[C_CANDN] = 0;
+      c[C_GROWN_OUT] = 0;
+      c[C_GROWN_IN] = 0;
+    }
+  }
+  __syncthreads();
+  if (s_skip) {
+    if (tid == 0) cudaGraphSetConditional(repair, 0u);
+    return;
+  }
+  const void *data = data_base + s_off;
+  const uint64_t n = s_n < SMALL_EDGES ? s_n : SMALL_EDGES;
+  const uint64_t nops = directed ? n : 2 * n;
+  const int weighted = W ? 1 : 0;
+  if (s_pairs) {
+    const uint64_t *p = reinterpret_cast<const uint64_t *>(data);
+    for (uint64_t i = tid; i < n; i += FS_TPB) {
+      uint64_t s64 = __ldcv(&p[2 * i]), d64 = __ldcv(&p[2 * i + 1]);
+      uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
+      sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, w, directed);
+    }
+  } else {
+    const uint64_t *e = reinterpret_cast<const uint64_t *>(data);
+    for (uint64_t i = tid; i < n; i += FS_TPB) {
+      uint64_t s64 = __ldcv(&e[3 * i]), d64 = __ldcv(&e[3 * i + 1]), w64 = __ldcv(&e[3 * i + 2]);
+      sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, weighted ? (uint32_t)w64 : 0u, directed);
+    }
+  }
+  __syncthreads();
+  for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::lookup_op(g, ops, j, add);
+  __syncthreads();
+  if (add) {
+    // each warp grows its own vertices (a vertex is in a grow list once); the
+    // copies of long lists (a hub's) are left to the whole CTA below
+    constexpr unsigned BIG = 16;
+    __shared__ sdev::GrowClaim s_big[BIG];
+    __shared__ int s_big_in[BIG];
+    __shared__ unsigned s_nbig;
+    if (tid == 0) s_nbig = 0;
+    __syncthreads();
+    const unsigned gw = tid >> 5, gl = tid & 31;
+    for (int in = 0; in < (g.symmetric ? 1 : 2); in++) {
+      const DevDir &dir = in ? g.in : g.out;
+      const unsigned long long nv = c[in ? C_GROWN_IN : C_GROWN_OUT];
+      for (unsigned long long k = gw; k < nv; k += FS_TPB / 32) {
+        const uint32_t v = dir.grow[k];
+        // a slot may be free (taken below, or the warp copies after all);
+        // lane 0's view keeps the choice uniform across the warp
+        const bool more = __shfl_sync(FULL, s_nbig < BIG ? 1 : 0, 0) != 0;
+        sdev::GrowClaim cl;
+        if (sdev::grow_vertex_warp<W>(dir, c, v, gl, more, &cl)) {
+          unsigned slot = 0;
+          if (gl == 0) slot = atomicAdd(&s_nbig, 1u);
+          slot = __shfl_sync(FULL, slot, 0);
+          if (slot < BIG) {
+            if (gl == 0) {
+              s_big[slot] = cl;
+              s_big_in[slot] = in;
+            }
+          } else {
+            sdev::grow_copy<W>(dir, cl, gl, 32);
+            __syncwarp();
+            if (gl == 0) sdev::grow_publish(dir, cl);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    const unsigned nbig = s_nbig < BIG ? s_nbig : BIG;
+    for (unsigned b = 0; b < nbig; b++) sdev::grow_copy<W>(s_big_in[b] ? g.in : g.out, s_big[b], tid, FS_TPB);
+    __syncthreads();
+    if (tid < nbig) sdev::grow_publish(s_big_in[tid] ? g.in : g.out, s_big[tid]);
+  }
+  __syncthreads();
+  if (c[C_ERR]) {
+    if (tid == 0) cudaGraphSetConditional(repair, 0u);
+    return;
+  }
+  if (add) {
+    for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::write_new_op<W>(g, ops, j);
+    __syncthreads();
+  }
+  for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::count_op<W>(g, ops, j, add);
+  __syncthreads();
+  for (uint64_t i = tid; i < n; i += FS_TPB) sdev::edge_old(ops, i, directed, add, 1, s_want ? old_host : nullptr, cand, c);
+  __syncthreads();
+  const uint64_t ncand = c[C_CANDN];
+  const uint64_t warp = tid >> 5, nwarps = FS_TPB / 32;
+  if (add) {
+    unsigned long long local = seed_add<A>(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], mst, warp, nwarps);
+    warp_add_result(local, &c[C_RESULT]);
+  } else {
+    seed_del(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], warp, nwarps);
+  }
+  __syncthreads();
+  bool over = false;
+  if (c[C_QN0] && !c[C_ERR]) {
+    if (!add) over = del_tiny_levels<A, W>(g, q0, fr.q1, fr.tree, fr.limit, fr.big, fr.max_iter, mst);
+    if (!over && fr.tiny_edges && c[C_QN0])
+      tiny_levels<A, W>(g, q0, &c[C_QN0], fr.q1, &c[C_QN1], q0, &c[C_QN0], fr.max_levels, fr.tiny_edges, mst, false);
+  }
+  if (tid == 0) {
+    c[C_OVER] = over ? 1 : 0;
+    cudaGraphSetConditional(repair, (over || (c[C_QN0] && !c[C_ERR])) ? 1u : 0u);
   }
 }
 
@@ -2293,9 +2379,12 @@ int add_level_loop(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
 //       k_inv_begin ; k_rescue ; k_expand     (queue 1 -> 0)
 //       k_inv_cond }
 //     k_reset ; k_pull ; k_copy_frontier (reset set -> queue 0 for the push loop) }
-// *out is the IF node.
+// *out is the IF node.  With `fused` (the fused apply kernel ran the one-CTA
+// repair and left its hand-over decision in C_OVER) the first node is
+// k_handover instead of k_del_tiny.
 template <int A, bool W>
-int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps, cudaGraphNode_t *out) {
+int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps, cudaGraphNode_t *out,
+                   bool fused = false) {
   if (!g.cap_stream) RG_CUDA(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
   const uint64_t big = recompute_threshold(g);
   const uint64_t limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
@@ -2310,11 +2399,12 @@ int add_del_repair(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
     int in_graph = 1;
     void *ta[] = {(void *)&g.d, (void *)&q0, (void *)&q1, (void *)&tr, (void *)&limit, (void *)&big,
                   (void *)&max_iter, (void *)&mst, (void *)&th, (void *)&in_graph};
+    void *hoa[] = {(void *)&g.d, (void *)&th};
     cudaKernelNodeParams tp = {};
-    tp.func = (void *)k_del_tiny<A, W>;
+    tp.func = fused ? (void *)k_handover : (void *)k_del_tiny<A, W>;
     tp.gridDim = dim3(1);
-    tp.blockDim = dim3(DT_TPB);
-    tp.kernelParams = ta;
+    tp.blockDim = dim3(fused ? 1 : DT_TPB);
+    tp.kernelParams = fused ? hoa : ta;
     cudaGraphNode_t tn;
     if ((e = cudaGraphAddKernelNode(&tn, graph, deps, ndeps, &tp)) != cudaSuccess) break;
     cudaGraphNodeParams ip = {};
@@ -2738,8 +2828,9 @@ int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t
 }
 
 // One fused apply phase as graph nodes: k_apply_small (reading the header at
-// hdr_off of the staging buffer) -> IF (frontier) { [deletion repair ->] level
-// loop }.  *out is the IF node.
+// hdr_off of the staging buffer; it runs small repairs itself) -> IF (work is
+// left) { [k_handover -> IF (its deletion repair handed over) { grid-wide
+// deletion repair } ->] level loop }.  *out is the IF node.
 template <int A, bool W>
 int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps,
                     cudaGraphConditionalHandle ih, bool add, int directed, uint64_t hdr_off, int second,
@@ -2753,16 +2844,26 @@ int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, si
   int a_add = add ? 1 : 0, a_dir = directed ? 1 : 0, a_second = second;
   uint32_t *q0 = g.q[0];
   uint32_t mst = mod_stamp(g);
+  FusedRepair fr = {};
+  fr.q1 = g.q[1];
+  fr.tree = g.tree;
+  fr.limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
+  fr.big = recompute_threshold(g);
+  fr.max_iter = (uint64_t)g.V + 2;
+  fr.max_levels = cfg.max_levels;
+  fr.tiny_edges = cfg.tiny_edges;
+  cudaError_t e = cudaSuccess;
   void *args[] = {(void *)&g.d,  (void *)&ops, (void *)&hdr, (void *)&data,     (void *)&old_host, (void *)&cand,
-                  (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&a_second, (void *)&ih};
+                  (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&a_second, (void *)&ih,
+                  (void *)&fr};
   cudaKernelNodeParams kp = {};
   kp.func = (void *)k_apply_small<A, W>;
   kp.gridDim = dim3(1);
   kp.blockDim = dim3(FS_TPB);
   kp.kernelParams = args;
   cudaGraphNode_t kn;
-  cudaError_t e = cudaGraphAddKernelNode(&kn, graph, deps, ndeps, &kp);
-  if (e != cudaSuccess) return cuda_fail(e, "building the fused apply graph");
+  if ((e = cudaGraphAddKernelNode(&kn, graph, deps, ndeps, &kp)) != cudaSuccess)
+    return cuda_fail(e, "building the fused apply graph");
   cudaGraphNodeParams ip = {};
   ip.type = cudaGraphNodeTypeConditional;
   ip.conditional.handle = ih;
@@ -2772,7 +2873,7 @@ int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, si
   cudaGraph_t body = ip.conditional.phGraph_out[0];
   cudaGraphNode_t last, loop;
   if (add) return add_level_loop<A, W>(g, body, nullptr, 0, cfg, &loop);
-  int rc = add_del_repair<A, W>(g, body, nullptr, 0, &last);
+  int rc = add_del_repair<A, W>(g, body, nullptr, 0, &last, true);
   if (!rc) rc = add_level_loop<A, W>(g, body, &last, 1, cfg, &loop);
   return rc;
 }
@@ -2828,8 +2929,7 @@ int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
 }
 
 // Fused small-batch apply graph per (algorithm, weighting, add/delete,
-// directed): k_apply_small -> IF (frontier) { [deletion repair ->] level loop }
-// -> control block to the host.  Its parameters hold the op, staging and pool
+// directed): the nodes of add_apply_phase -> control block to the host.  Its parameters hold the op, staging and pool
 // addresses, so it is rebuilt when any of them moves.
 template <int A, bool W>
 int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
