@@ -71,6 +71,7 @@ enum Ctl : int {
   C_HVE = 28,      // ... by the expand pass
   C_HVP = 29,      // ... by the pull over the reset set
   C_OVER = 30,     // the fused apply's one-CTA deletion repair handed over to the grid-wide one
+  C_LEFT = 31,     // what the insert+delete kernel left to the graph (1: insert loop and delete batch, 2: delete repair)
   C_COUNT = 32
 };
 
@@ -219,8 +220,10 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t *q, 
 // Header of a small update batch in the graph's mapped pinned staging buffer,
 // read by the fused apply kernel.  A submission holds up to two headers (an
 // insert batch at offset 0, a delete batch at APPLY_HDR2); the edges follow at
-// APPLY_DATA_OFF + data_off, and the per-edge old counts of a single batch are
-// written back at apply_old_off().
+// APPLY_DATA_OFF + data_off (0, or apply_data2_off() for the delete batch of
+// an insert+delete submission: fixed, so that the kernel reads the edges
+// without waiting for the header), and the per-edge old counts of a single
+// batch are written back at apply_old_off().
 struct ApplyHdr {
   uint64_t n;         // edges in the batch
   uint64_t pairs;     // 1: reference-format (src,dst) pairs, 0: rg_edge records
@@ -232,6 +235,8 @@ constexpr uint64_t APPLY_HDR2 = 64;
 constexpr uint64_t APPLY_DATA_OFF = 128;
 constexpr uint64_t SMALL_EDGES = 2048;  // largest batch of the fused single-CTA apply path
 inline uint64_t apply_old_off() { return APPLY_DATA_OFF + 2 * SMALL_EDGES * sizeof(rg_edge); }
+// the delete batch of an insert+delete submission starts here, from APPLY_DATA_OFF
+inline uint64_t apply_data2_off() { return SMALL_EDGES * sizeof(rg_edge); }
 
 // A node of the versioned label history (rg_history.cu).
 struct HistNode {

@@ -1837,12 +1837,41 @@ struct FusedRepair {
   uint64_t tiny_edges;  // out-slot limit of an in-place push level (0: none in place)
 };
 
+// A batch's header as the fused kernels read it.
+struct StagedBatch {
+  uint64_t n, pairs, want, inv_tag;
+};
+
+// The batch crosses the bus in 16-byte loads into device scratch: the first
+// APPLY_SPEC chunks in the same round trip as the header (thread hdr_t reads
+// the header, threads chunk_t .. chunk_t + APPLY_SPEC - 1 the chunks), the
+// rest in apply_batch once the header gives the size.  The host wrote both
+// before the launch; they are read past any cache.
+constexpr unsigned APPLY_SPEC = 256;
+
+__device__ __forceinline__ void stage_batch(const ApplyHdr *hdr, const char *data, uint4 *scratch, StagedBatch &sb,
+                                            unsigned hdr_t, unsigned chunk_t) {
+  const unsigned tid = threadIdx.x;
+  const uint4 *raw = reinterpret_cast<const uint4 *>(data);
+  if (tid >= chunk_t && tid < chunk_t + APPLY_SPEC) scratch[tid - chunk_t] = __ldcv(&raw[tid - chunk_t]);
+  if (tid == hdr_t) {
+    sb.n = __ldcv(&hdr->n);
+    sb.pairs = __ldcv(&hdr->pairs);
+    sb.want = __ldcv(&hdr->want_old);
+    sb.inv_tag = __ldcv(&hdr->inv_tag);
+  }
+}
+
+// One staged batch through the storage steps, the seeding and the in-place
+// repair, by all threads of the CTA after a barrier.  Returns 0 when nothing
+// is left, 1 when the repair left work for the graph nodes after the kernel
+// (C_OVER set when the deletion repair handed over), 2 after a storage error
+// or when it skipped the batch.
 template <int A, bool W>
-__global__ void __launch_bounds__(FS_TPB)
-    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data_base, uint64_t *old_host,
-                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
-                  cudaGraphConditionalHandle repair, FusedRepair fr) {
-  __shared__ uint64_t s_n, s_pairs, s_want, s_off;
+__device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, const StagedBatch &sb,
+                                           const char *data, uint64_t *old_host, uint32_t *cand, int add, int directed,
+                                           uint32_t *q0, uint32_t mst, int second, const FusedRepair &fr,
+                                           uint4 *scratch) {
   __shared__ int s_skip;
   unsigned long long *c = g.ctl;
   const unsigned tid = threadIdx.x;
@@ -1850,13 +1879,8 @@ __global__ void __launch_bounds__(FS_TPB)
     // the second batch of a submission does nothing after an error in the first
     s_skip = second && c[C_ERR] != 0;
     if (!s_skip) {
-      // the host wrote the header before the launch; read it past any cache
-      s_n = __ldcv(&hdr->n);
-      s_pairs = __ldcv(&hdr->pairs);
-      s_want = __ldcv(&hdr->want_old);
-      s_off = __ldcv(&hdr->data_off);
       const unsigned long long kl = c[C_KLAUNCH];
-      prologue_ctl(c, __ldcv(&hdr->inv_tag));
+      prologue_ctl(c, sb.inv_tag);
       if (second) c[C_KLAUNCH] = kl;  // the count covers the whole submission
       c[C_CANDN] = 0;
       c[C_GROWN_OUT] = 0;
@@ -1864,25 +1888,27 @@ __global__ void __launch_bounds__(FS_TPB)
     }
   }
   __syncthreads();
-  if (s_skip) {
-    if (tid == 0) cudaGraphSetConditional(repair, 0u);
-    return;
-  }
-  const void *data = data_base + s_off;
-  const uint64_t n = s_n < SMALL_EDGES ? s_n : SMALL_EDGES;
+  if (s_skip) return 2;
+  const uint64_t n = sb.n < SMALL_EDGES ? sb.n : SMALL_EDGES;
   const uint64_t nops = directed ? n : 2 * n;
   const int weighted = W ? 1 : 0;
-  if (s_pairs) {
-    const uint64_t *p = reinterpret_cast<const uint64_t *>(data);
+  const uint64_t chunks = (n * (sb.pairs ? 16 : sizeof(rg_edge)) + 15) / 16;
+  if (chunks > APPLY_SPEC) {
+    const uint4 *raw = reinterpret_cast<const uint4 *>(data);
+    for (uint64_t k = APPLY_SPEC + tid; k < chunks; k += FS_TPB) scratch[k] = __ldcv(&raw[k]);
+    __syncthreads();
+  }
+  if (sb.pairs) {
+    const uint64_t *p = reinterpret_cast<const uint64_t *>(scratch);
     for (uint64_t i = tid; i < n; i += FS_TPB) {
-      uint64_t s64 = __ldcv(&p[2 * i]), d64 = __ldcv(&p[2 * i + 1]);
+      uint64_t s64 = __ldcg(&p[2 * i]), d64 = __ldcg(&p[2 * i + 1]);
       uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
       sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, w, directed);
     }
   } else {
-    const uint64_t *e = reinterpret_cast<const uint64_t *>(data);
+    const uint64_t *e = reinterpret_cast<const uint64_t *>(scratch);
     for (uint64_t i = tid; i < n; i += FS_TPB) {
-      uint64_t s64 = __ldcv(&e[3 * i]), d64 = __ldcv(&e[3 * i + 1]), w64 = __ldcv(&e[3 * i + 2]);
+      uint64_t s64 = __ldcg(&e[3 * i]), d64 = __ldcg(&e[3 * i + 1]), w64 = __ldcg(&e[3 * i + 2]);
       sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, weighted ? (uint32_t)w64 : 0u, directed);
     }
   }
@@ -1932,17 +1958,14 @@ __global__ void __launch_bounds__(FS_TPB)
     if (tid < nbig) sdev::grow_publish(s_big_in[tid] ? g.in : g.out, s_big[tid]);
   }
   __syncthreads();
-  if (c[C_ERR]) {
-    if (tid == 0) cudaGraphSetConditional(repair, 0u);
-    return;
-  }
+  if (c[C_ERR]) return 2;
   if (add) {
     for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::write_new_op<W>(g, ops, j);
     __syncthreads();
   }
   for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::count_op<W>(g, ops, j, add);
   __syncthreads();
-  for (uint64_t i = tid; i < n; i += FS_TPB) sdev::edge_old(ops, i, directed, add, 1, s_want ? old_host : nullptr, cand, c);
+  for (uint64_t i = tid; i < n; i += FS_TPB) sdev::edge_old(ops, i, directed, add, 1, sb.want ? old_host : nullptr, cand, c);
   __syncthreads();
   const uint64_t ncand = c[C_CANDN];
   const uint64_t warp = tid >> 5, nwarps = FS_TPB / 32;
@@ -1959,10 +1982,55 @@ __global__ void __launch_bounds__(FS_TPB)
     if (!over && fr.tiny_edges && c[C_QN0])
       tiny_levels<A, W>(g, q0, &c[C_QN0], fr.q1, &c[C_QN1], q0, &c[C_QN0], fr.max_levels, fr.tiny_edges, mst, false);
   }
-  if (tid == 0) {
-    c[C_OVER] = over ? 1 : 0;
-    cudaGraphSetConditional(repair, (over || (c[C_QN0] && !c[C_ERR])) ? 1u : 0u);
+  const bool left = over || (c[C_QN0] && !c[C_ERR]);
+  __syncthreads();  // every thread has read the counts before the next batch resets them
+  if (tid == 0) c[C_OVER] = over ? 1 : 0;
+  return left ? 1 : 0;
+}
+
+template <int A, bool W>
+__global__ void __launch_bounds__(FS_TPB)
+    k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data, uint64_t *old_host,
+                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
+                  cudaGraphConditionalHandle repair, FusedRepair fr, uint4 *scratch) {
+  __shared__ StagedBatch sb;
+  stage_batch(hdr, data, scratch, sb, 0, 32);
+  __syncthreads();
+  const int r = apply_batch<A, W>(g, ops, sb, data, old_host, cand, add, directed, q0, mst, second, fr, scratch);
+  if (threadIdx.x == 0) cudaGraphSetConditional(repair, r == 1 ? 1u : 0u);
+}
+
+// An insert batch and then a delete batch in one kernel (both staged in one
+// round trip): the delete batch runs here too when the insert batch's repair
+// finished in place.  C_LEFT tells the IF body after the kernel what is left:
+// 1 the insert batch's level loop and then the whole delete batch, 2 the
+// delete batch's repair.
+template <int A, bool W>
+__global__ void __launch_bounds__(FS_TPB)
+    k_apply_mixed(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr1, const char *data1, const ApplyHdr *hdr2,
+                  const char *data2, uint32_t *cand, int directed, uint32_t *q0, uint32_t mst,
+                  cudaGraphConditionalHandle left, FusedRepair fr, uint4 *scratch1, uint4 *scratch2) {
+  __shared__ StagedBatch sb1, sb2;
+  stage_batch(hdr1, data1, scratch1, sb1, 0, 32);
+  stage_batch(hdr2, data2, scratch2, sb2, 32 + APPLY_SPEC, 64 + APPLY_SPEC);
+  __syncthreads();
+  int r = apply_batch<A, W>(g, ops, sb1, data1, nullptr, cand, 1, directed, q0, mst, 0, fr, scratch1);
+  unsigned long long lf = r == 1 ? 1 : 0;
+  if (r == 0) {
+    r = apply_batch<A, W>(g, ops, sb2, data2, nullptr, cand, 0, directed, q0, mst, 1, fr, scratch2);
+    lf = r == 1 ? 2 : 0;
   }
+  if (threadIdx.x == 0) {
+    g.ctl[C_LEFT] = lf;
+    cudaGraphSetConditional(left, lf ? 1u : 0u);
+  }
+}
+
+// Selects the SWITCH case of the IF body after k_apply_mixed.
+__global__ void k_left(DevGraph g, cudaGraphConditionalHandle sw) {
+  const unsigned long long lf = g.ctl[C_LEFT];
+  g.ctl[C_KLAUNCH] += lf == 1 ? 2 : 1;  // this kernel, and the delete batch's own kernel in case 1
+  cudaGraphSetConditional(sw, (unsigned)lf);
 }
 
 // need_update_tree_add (core/graph.hpp:987-1000) / need_update_tree_del
@@ -2827,6 +2895,18 @@ int tree_del(Graph &g, uint64_t n_edges, int directed, bool from_cands, uint64_t
   return rc;
 }
 
+FusedRepair fused_repair(const Graph &g, const LevelCfg &cfg) {
+  FusedRepair fr = {};
+  fr.q1 = g.q[1];
+  fr.tree = g.tree;
+  fr.limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
+  fr.big = recompute_threshold(g);
+  fr.max_iter = (uint64_t)g.V + 2;
+  fr.max_levels = cfg.max_levels;
+  fr.tiny_edges = cfg.tiny_edges;
+  return fr;
+}
+
 // One fused apply phase as graph nodes: k_apply_small (reading the header at
 // hdr_off of the staging buffer; it runs small repairs itself) -> IF (work is
 // left) { [k_handover -> IF (its deletion repair handed over) { grid-wide
@@ -2838,24 +2918,18 @@ int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, si
   sdev::OpView ops = sdev::op_view(g);
   char *base = reinterpret_cast<char *>(g.stage_host_dev);
   const ApplyHdr *hdr = reinterpret_cast<const ApplyHdr *>(base + hdr_off);
-  const char *data = base + APPLY_DATA_OFF;
+  const char *data = base + APPLY_DATA_OFF + (second ? apply_data2_off() : 0);
   uint64_t *old_host = reinterpret_cast<uint64_t *>(base + apply_old_off());
+  uint4 *scratch = reinterpret_cast<uint4 *>(g.stage_dev);
   uint32_t *cand = op_cand(g);
   int a_add = add ? 1 : 0, a_dir = directed ? 1 : 0, a_second = second;
   uint32_t *q0 = g.q[0];
   uint32_t mst = mod_stamp(g);
-  FusedRepair fr = {};
-  fr.q1 = g.q[1];
-  fr.tree = g.tree;
-  fr.limit = (uint64_t)((double)g.V * 0.1);  // has_parents guard, core/graph.hpp:1900
-  fr.big = recompute_threshold(g);
-  fr.max_iter = (uint64_t)g.V + 2;
-  fr.max_levels = cfg.max_levels;
-  fr.tiny_edges = cfg.tiny_edges;
+  FusedRepair fr = fused_repair(g, cfg);
   cudaError_t e = cudaSuccess;
   void *args[] = {(void *)&g.d,  (void *)&ops, (void *)&hdr, (void *)&data,     (void *)&old_host, (void *)&cand,
                   (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&a_second, (void *)&ih,
-                  (void *)&fr};
+                  (void *)&fr,   (void *)&scratch};
   cudaKernelNodeParams kp = {};
   kp.func = (void *)k_apply_small<A, W>;
   kp.gridDim = dim3(1);
@@ -2880,11 +2954,15 @@ int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, si
 
 uint64_t apply_key(const Graph &g, const LevelCfg &cfg) {
   return splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
-         splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^ cfg_key(cfg) ^ splitmix64(recompute_threshold(g) + 11);
+         splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^ splitmix64((uint64_t)(uintptr_t)g.stage_dev + 13) ^
+         cfg_key(cfg) ^ splitmix64(recompute_threshold(g) + 11);
 }
 
-// Insert batch then delete batch in one graph: phase 1 (header 1) -> phase 2
-// (header 2, skipped after an error in phase 1) -> control block to the host.
+// Insert batch then delete batch in one graph: k_apply_mixed (both batches,
+// and their repairs while they stay small) -> IF (work is left) { k_left ->
+// SWITCH { 1: level loop -> the delete batch's phase (add_apply_phase, skipped
+// after an error in the insert batch) | 2: the rest of the delete batch's
+// repair } } -> control block to the host.
 template <int A, bool W>
 int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
   LoopGraph &slot = g.mixes[(A * 2 + (W ? 1 : 0)) * 2 + (directed ? 1 : 0)];
@@ -2903,13 +2981,68 @@ int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
   int rc = RG_OK;
   cudaError_t e = cudaSuccess;
   do {
-    cudaGraphConditionalHandle h1, h2;
-    if ((e = cudaGraphConditionalHandleCreate(&h1, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    if ((e = cudaGraphConditionalHandleCreate(&h2, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    cudaGraphNode_t if1, if2, mn;
-    if ((rc = add_apply_phase<A, W>(g, graph, nullptr, 0, h1, true, directed, 0, 0, cfg, &if1))) break;
-    if ((rc = add_apply_phase<A, W>(g, graph, &if1, 1, h2, false, directed, APPLY_HDR2, 1, cfg, &if2))) break;
-    if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &if2, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
+    cudaGraphConditionalHandle hl;
+    if ((e = cudaGraphConditionalHandleCreate(&hl, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    sdev::OpView ops = sdev::op_view(g);
+    char *base = reinterpret_cast<char *>(g.stage_host_dev);
+    const ApplyHdr *hdr1 = reinterpret_cast<const ApplyHdr *>(base), *hdr2 =
+                                                                         reinterpret_cast<const ApplyHdr *>(base + APPLY_HDR2);
+    const char *data1 = base + APPLY_DATA_OFF, *data2 = base + APPLY_DATA_OFF + apply_data2_off();
+    uint4 *scr1 = reinterpret_cast<uint4 *>(g.stage_dev);
+    uint4 *scr2 = reinterpret_cast<uint4 *>(reinterpret_cast<char *>(g.stage_dev) + apply_data2_off());
+    uint32_t *cand = op_cand(g), *q0 = g.q[0];
+    int a_dir = directed ? 1 : 0;
+    uint32_t mst = mod_stamp(g);
+    FusedRepair fr = fused_repair(g, cfg);
+    void *args[] = {(void *)&g.d,   (void *)&ops, (void *)&hdr1, (void *)&data1, (void *)&hdr2, (void *)&data2,
+                    (void *)&cand,  (void *)&a_dir, (void *)&q0, (void *)&mst,   (void *)&hl,   (void *)&fr,
+                    (void *)&scr1, (void *)&scr2};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *)k_apply_mixed<A, W>;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(FS_TPB);
+    kp.kernelParams = args;
+    cudaGraphNode_t kn;
+    if ((e = cudaGraphAddKernelNode(&kn, graph, nullptr, 0, &kp)) != cudaSuccess) break;
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hl;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t ifn;
+    if ((e = cudaGraphAddNode(&ifn, graph, &kn, 1, &ip)) != cudaSuccess) break;
+    cudaGraph_t body = ip.conditional.phGraph_out[0];
+    cudaGraphConditionalHandle sw;
+    if ((e = cudaGraphConditionalHandleCreate(&sw, body, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    void *la[] = {(void *)&g.d, (void *)&sw};
+    cudaKernelNodeParams lp = {};
+    lp.func = (void *)k_left;
+    lp.gridDim = dim3(1);
+    lp.blockDim = dim3(1);
+    lp.kernelParams = la;
+    cudaGraphNode_t ln;
+    if ((e = cudaGraphAddKernelNode(&ln, body, nullptr, 0, &lp)) != cudaSuccess) break;
+    cudaGraphNodeParams sp = {};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = sw;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = 3;
+    cudaGraphNode_t sn;
+    if ((e = cudaGraphAddNode(&sn, body, &ln, 1, &sp)) != cudaSuccess) break;
+    // case 1: the insert batch's level loop, then the delete batch as its own phase
+    cudaGraph_t c1 = sp.conditional.phGraph_out[1];
+    cudaGraphNode_t loop1, ph2;
+    if ((rc = add_level_loop<A, W>(g, c1, nullptr, 0, cfg, &loop1))) break;
+    cudaGraphConditionalHandle h3;
+    if ((e = cudaGraphConditionalHandleCreate(&h3, c1, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+    if ((rc = add_apply_phase<A, W>(g, c1, &loop1, 1, h3, false, directed, APPLY_HDR2, 1, cfg, &ph2))) break;
+    // case 2: the rest of the delete batch's repair
+    cudaGraph_t c2 = sp.conditional.phGraph_out[2];
+    cudaGraphNode_t rep2, loop2;
+    if ((rc = add_del_repair<A, W>(g, c2, nullptr, 0, &rep2, true))) break;
+    if ((rc = add_level_loop<A, W>(g, c2, &rep2, 1, cfg, &loop2))) break;
+    cudaGraphNode_t mn;
+    if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &ifn, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
                                       cudaMemcpyDeviceToHost)) != cudaSuccess)
       break;
     e = cudaGraphInstantiate(&slot.exec, graph, 0);
@@ -3031,9 +3164,9 @@ int apply_add_del_t(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge
   char *st = reinterpret_cast<char *>(g.stage_host);
   ApplyHdr *h1 = reinterpret_cast<ApplyHdr *>(st), *h2 = reinterpret_cast<ApplyHdr *>(st + APPLY_HDR2);
   std::memcpy(st + APPLY_DATA_OFF, adds, n_add * sizeof(rg_edge));
-  std::memcpy(st + APPLY_DATA_OFF + n_add * sizeof(rg_edge), dels, n_del * sizeof(rg_edge));
+  std::memcpy(st + APPLY_DATA_OFF + apply_data2_off(), dels, n_del * sizeof(rg_edge));
   *h1 = ApplyHdr{n_add, 0, 0, 0, 0};
-  *h2 = ApplyHdr{n_del, 0, 0, 0, n_add * sizeof(rg_edge)};
+  *h2 = ApplyHdr{n_del, 0, 0, 0, apply_data2_off()};
   g.adj_version++;
   if ((rc = guard_counters(g))) return rc;
   if (++g.inv_epoch >= 0x7FFFFFFFu) {
@@ -3045,7 +3178,7 @@ int apply_add_del_t(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge
   reset_stats(g);
   cudaGraphExec_t exec;
   if ((rc = mixed_exec<A, W>(g, directed, &exec))) return rc;
-  count_launch(g, 2);
+  count_launch(g);
   RG_CUDA(cudaGraphLaunch(exec, g.stream));
   RG_CUDA(cudaStreamSynchronize(g.stream));
   if (g.h_ctl[C_ERR] == RG_ENOSPACE && g.h_ctl[C_AUX] == 1) {
