@@ -113,7 +113,7 @@ int rg_apply_del(rg_graph *g, int algo, const rg_edge *edges, uint64_t n, int di
 
 /* One step of src/sssp_inc_batch.cpp:141-175: rg_apply_add of `adds`, then
  * rg_apply_del of `dels`, as one device submission with one synchronisation
- * when both batches hold at most RG_OPT_FUSED_MAX edges (default 1024; two
+ * when both batches hold at most RG_OPT_FUSED_MAX edges (default 2048; two
  * submissions otherwise). */
 int rg_apply_add_del(rg_graph *g, int algo, const rg_edge *adds, uint64_t n_add, const rg_edge *dels, uint64_t n_del,
                      int directed);
@@ -213,7 +213,7 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
  *                         groups - 1 launches of about equal entries; each launch
  *                         reads the values the earlier ones set in this level.
  *   RG_OPT_FUSED_MAX      update batches of at most this many edges (0..2048,
- *                         default 1024) take the fused single-CTA path of
+ *                         default 2048) take the fused single-CTA path of
  *                         rg_apply_*: storage and small repairs in one
  *                         submission; larger batches run grid-wide kernels. */
 typedef enum {

@@ -318,7 +318,7 @@ struct Graph {
   uint64_t max_levels = 0;  // bound on the levels of one tree call (0: 4 |V| + 1024)
   // largest batch of the fused single-CTA apply path (<= SMALL_EDGES); measured on RMAT-24
   // SSSP, larger batches run faster on the grid-wide kernels
-  uint64_t fused_max = 1024;
+  uint64_t fused_max = 2048;
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]

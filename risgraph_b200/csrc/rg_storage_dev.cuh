@@ -64,7 +64,9 @@ __device__ __forceinline__ void unpack_pair(const uint64_t *p, uint64_t i, int d
 
 // Find the record of op j's (s,d,w); create it (and reserve its slots at the
 // end of the src / dst segments) when `create`.  Vertices whose segment just
-// ran out of capacity go to the direction's grow list.
+// ran out of capacity go to the direction's grow list.  Lanes of a warp that
+// reserve slots of the same vertex together take consecutive slots with one
+// atomic (a hub is the source of many edges of one batch).
 __device__ __forceinline__ void lookup_op(const DevGraph &g, OpView ops, uint64_t j, int create) {
   uint32_t s = ops.src[j], d = ops.dst[j], w = ops.w[j];
   if (ops.mul[j] == 0) { ops.rid[j] = UNSET; ops.flag[j] = 0; return; }
@@ -79,8 +81,13 @@ __device__ __forceinline__ void lookup_op(const DevGraph &g, OpView ops, uint64_
       if (mine == UNSET) {
         // (no fence before the claim below: a thread that finds this record
         // in the index only takes its id; the record's fields are read after
-        // the kernel or CTA barrier that ends the lookup step)
-        unsigned long long r = atomicAdd(g.rec_top, 1ull);
+        // the kernel or CTA barrier that ends the lookup step).  The lanes
+        // that claim together take their ids with one atomic.
+        const unsigned m = __activemask();
+        const int leader = __ffs(m) - 1, lane = threadIdx.x & 31;
+        unsigned long long r = 0;
+        if (lane == leader) r = atomicAdd(g.rec_top, (unsigned long long)__popc(m));
+        r = __shfl_sync(m, r, leader) + __popc(m & ((1u << lane) - 1));
         if (r >= g.rec_cap) { set_err(g.ctl, RG_ENOSPACE); break; }
         mine = (uint32_t)r;
         g.rec_num[mine] = 0;
@@ -102,16 +109,27 @@ __device__ __forceinline__ void lookup_op(const DevGraph &g, OpView ops, uint64_
   ops.rid[j] = rid;
   ops.flag[j] = created;
   if (created) {
-    uint32_t po = atomicAdd(&g.out.len[s], 1u);
+    // both directions' slots are reserved before either result is used, so
+    // that the two atomics are in flight together
+    const unsigned am = __activemask();
+    const int lane = threadIdx.x & 31;
+    const unsigned mo = __match_any_sync(am, s), mi = g.symmetric ? 0u : __match_any_sync(am, d);
+    const int lo = __ffs(mo) - 1, li = __ffs(mi) - 1;
+    uint32_t bo = 0, bi = 0;
+    if (lane == lo) bo = atomicAdd(&g.out.len[s], (uint32_t)__popc(mo));
+    if (!g.symmetric && lane == li) bi = atomicAdd(&g.in.len[d], (uint32_t)__popc(mi));
+    const uint32_t co = g.out.cap[s], ci = g.symmetric ? 0u : g.in.cap[d];
+    const unsigned lt = (1u << lane) - 1;
+    const uint32_t po = __shfl_sync(mo, bo, lo) + __popc(mo & lt);
     g.rec_out[rid] = po;
-    if (po == g.out.cap[s]) {
+    if (po == co) {
       unsigned long long k = atomicAdd(&g.ctl[C_GROWN_OUT], 1ull);
       g.out.grow[k] = s;
     }
     if (!g.symmetric) {
-      uint32_t pi = atomicAdd(&g.in.len[d], 1u);
+      const uint32_t pi = __shfl_sync(mi, bi, li) + __popc(mi & lt);
       g.rec_in[rid] = pi;
-      if (pi == g.in.cap[d]) {
+      if (pi == ci) {
         unsigned long long k = atomicAdd(&g.ctl[C_GROWN_IN], 1ull);
         g.in.grow[k] = d;
       }
@@ -179,26 +197,40 @@ struct GrowClaim {
   uint32_t new_cap, copy, old_cap, v;
 };
 
+// What vertex v's growth needs: *want slots (0 when v has room; a retry
+// after compaction skips vertices already grown), and the claim without its
+// new region.
+__device__ __forceinline__ GrowClaim grow_want(DevDir dir, uint32_t v, unsigned long long *want) {
+  GrowClaim cl = {0, 0, 0, 0, 0, v};
+  const uint32_t len = dir.len[v], cap = dir.cap[v];
+  *want = 0;
+  if (len > cap) {
+    uint64_t w = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
+    while (w < len) w *= 2;
+    if (w > 0xFFFFFFF0ull) w = 0xFFFFFFF0ull;
+    *want = w;
+    cl.from = dir.off[v];
+    cl.old_cap = cap;
+  }
+  cl.copy = len < cap ? len : cap;
+  return cl;
+}
+
 __device__ __forceinline__ GrowClaim grow_claim_warp(DevDir dir, unsigned long long *ctl, uint32_t v, int lane) {
   GrowClaim cl = {0, 0, 0, 0, 0, v};
   if (lane == 0) {
-    uint32_t len = dir.len[v], cap = dir.cap[v];
-    if (len > cap) {  // (a retry after compaction skips vertices already grown)
-      uint64_t want = cap ? (uint64_t)cap * 2 : (uint64_t)len + len / 8 + 2;
-      while (want < len) want *= 2;
-      if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
-      unsigned long long off = atomicAdd(dir.pool_top, (unsigned long long)want);
+    unsigned long long want;
+    cl = grow_want(dir, v, &want);
+    if (want) {
+      unsigned long long off = atomicAdd(dir.pool_top, want);
       if (off + want > dir.pool_cap) {
         atomicCAS(&ctl[C_ERR], 0ull, (unsigned long long)RG_ENOSPACE);
         ctl[C_AUX] = 1;
       } else {
         cl.new_cap = (uint32_t)want;
         cl.new_off = off;
-        cl.from = dir.off[v];
-        cl.old_cap = cap;
       }
     }
-    cl.copy = len < cap ? len : cap;
   }
   cl.new_cap = __shfl_sync(0xFFFFFFFFu, cl.new_cap, 0);
   cl.new_off = __shfl_sync(0xFFFFFFFFu, cl.new_off, 0);

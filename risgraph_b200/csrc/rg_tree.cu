@@ -77,6 +77,26 @@ __device__ __forceinline__ bool relax(const DevGraph &g, uint32_t u, uint64_t su
   return false;
 }
 
+// relax without the 4-byte value filter: the label itself is the first load,
+// so that an improving edge costs two round trips (load, CAS) instead of
+// three.  For latency-bound single-CTA levels, where the filter saves no
+// bandwidth worth having.
+template <int A>
+__device__ __forceinline__ bool relax_lab(const DevGraph &g, uint32_t u, uint64_t su, uint32_t v, uint32_t w) {
+  const uint64_t nv = Hook<A>::combine(su, w);
+  ulonglong2 cur = ld_lab(&g.lab[v]);
+  while (Hook<A>::better(nv, cur.x)) {
+    ulonglong2 want = make_ulonglong2(nv, pack_parent(u, w));
+    ulonglong2 old = cas128(&g.lab[v], cur, want);
+    if (old.x == cur.x && old.y == cur.y) {
+      mirror_improve<A>(g.val32, v, nv);
+      return true;
+    }
+    cur = old;
+  }
+  return false;
+}
+
 __device__ __forceinline__ void warp_add_result(unsigned long long local, unsigned long long *dst) {
   for (int o = 16; o; o >>= 1) local += __shfl_down_sync(FULL, local, o);
   if (lane_id() == 0 && local) atomicAdd(dst, local);
@@ -1055,7 +1075,7 @@ __device__ __forceinline__ void tiny_levels(const DevGraph &g, uint32_t *q_in, u
         const typename P_::E ent = __ldg(&pool[s_off[lo] + (e - s_pref[lo])]);
         v = P_::nbr(ent);
         scanned++;
-        if (!(v & DEAD)) upd = relax<A>(g, s_v[lo], s_su[lo], v, P_::wt(ent));
+        if (!(v & DEAD)) upd = relax_lab<A>(g, s_v[lo], s_su[lo], v, P_::wt(ent));
       }
       local += upd;
       const bool app = upd && atomicExch(&g.stamp[v], st) != st;
@@ -1099,7 +1119,9 @@ __global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_
 // host round trip happens between levels (the reference's driver decides
 // between levels on the host, core/graph.hpp:898-983, :1013-1111).
 
-__device__ __forceinline__ void prologue_ctl(unsigned long long *c, unsigned long long inv_tag) {
+// stamp: the control block's C_STAMP when the caller read it already.
+__device__ __forceinline__ void prologue_ctl(unsigned long long *c, unsigned long long inv_tag,
+                                             const unsigned long long *stamp = nullptr) {
   c[C_INVTAG] = inv_tag;
   c[C_INVITER] = 0;
   c[C_OVER] = 0;
@@ -1116,7 +1138,7 @@ __device__ __forceinline__ void prologue_ctl(unsigned long long *c, unsigned lon
   c[C_HVR] = 0;
   c[C_HVE] = 0;
   c[C_HVP] = 0;
-  c[C_STAMP] += 1;
+  c[C_STAMP] = (stamp ? *stamp : c[C_STAMP]) + 1;
 }
 
 __global__ void k_prologue(DevGraph g, unsigned long long inv_tag) { prologue_ctl(g.ctl, inv_tag); }
@@ -1345,14 +1367,18 @@ __global__ void k_seed_del(DevGraph g, const uint32_t *os, const uint32_t *od, c
 // tag.  The walk therefore stops at a vertex marked clear earlier in this
 // repair (chk == the repair's tag), and a clear walk marks the first vertices
 // of its chain, so that walks from their descendants end there.
+//
+// The three words of a step are loaded together, so that a step costs one
+// round trip to memory rather than three.
 __device__ __forceinline__ bool has_parents(const DevGraph &g, uint32_t x0, uint32_t tag_inv, uint64_t limit) {
   uint64_t num = 0;
   uint32_t x = x0;
   for (;;) {
-    if (ld_u32(&g.chk[x]) == tag_inv) break;
-    uint32_t t = ld_u32(&g.inv[x]);
+    const uint32_t ck = ld_u32(&g.chk[x]);
+    const uint32_t t = ld_u32(&g.inv[x]);
+    const uint32_t p = (uint32_t)ld_meta(&g.lab[x]);
+    if (ck == tag_inv) break;
     if (t == tag_inv || t == tag_inv + 1) return true;
-    uint32_t p = (uint32_t)ld_meta(&g.lab[x]);
     if (p == NONE) break;
     x = p;
     if (++num > limit) {
@@ -1402,10 +1428,12 @@ __device__ __forceinline__ void rescue_warps(const DevGraph &g, const uint32_t *
   const int lane = lane_id();
   for (uint64_t idx = warp; idx < n; idx += nwarps) {
     const uint32_t d = fin[idx];
-    if (ld_u32(&g.inv[d]) != tag_inv) continue;
+    // (the vertex's words in one round trip)
+    const uint32_t td = ld_u32(&g.inv[d]);
     const uint64_t sd = ld_v32(g.val32, d);
     const uint32_t len = seg_len(g.in, d);
     const uint64_t off = g.in.off[d];
+    if (td != tag_inv) continue;
     if (hv && len > HEAVY_DEG && queue_heavy(hv, hv_n, hv_cap, d, lane)) continue;
     for (uint32_t kb = 0; kb < len; kb += 32) {
       const uint32_t k = kb + lane;
@@ -1496,28 +1524,33 @@ __device__ __forceinline__ void expand_warps(const DevGraph &g, const uint32_t *
   const int lane = lane_id();
   for (uint64_t idx = warp; idx < n; idx += nwarps) {
     const uint32_t u = fin[idx];
-    if (ld_u32(&g.inv[u]) != tag_inv) continue;
-    if (lane == 0) {
-      unsigned long long k = atomicAdd(&g.ctl[C_TREEN], 1ull);
-      tree[k] = u;
-    }
+    // (the vertex's words in one round trip; its slot in the reset set is
+    // taken here and written after the scan, off the critical path)
+    const uint32_t tu = ld_u32(&g.inv[u]);
     const uint32_t len = seg_len(g.out, u);
     const uint64_t off = g.out.off[u];
-    if (hv && len > HEAVY_DEG && queue_heavy(hv, hv_n, hv_cap, u, lane)) continue;
-    for (uint32_t kb = 0; kb < len; kb += 32) {
-      const uint32_t k = kb + lane;
-      bool app = false;
-      uint32_t v = 0;
-      if (k < len) {
-        typename P::E e = pool[off + k];
-        v = P::nbr(e);
-        if (!(v & DEAD) && ld_meta(&g.lab[v]) == pack_parent(u, P::wt(e))) {
-          uint32_t t = ld_u32(&g.inv[v]);
-          if (t != tag_inv && t != tag_inv + 1) app = atomicCAS(&g.inv[v], t, tag_inv) == t;
+    if (tu != tag_inv) continue;
+    unsigned long long slot = 0;
+    if (lane == 0) slot = atomicAdd(&g.ctl[C_TREEN], 1ull);
+    if (!(hv && len > HEAVY_DEG && queue_heavy(hv, hv_n, hv_cap, u, lane))) {
+      for (uint32_t kb = 0; kb < len; kb += 32) {
+        const uint32_t k = kb + lane;
+        bool app = false;
+        uint32_t v = 0;
+        if (k < len) {
+          typename P::E e = pool[off + k];
+          v = P::nbr(e);
+          if (!(v & DEAD)) {
+            const uint64_t meta = ld_meta(&g.lab[v]);
+            const uint32_t t = ld_u32(&g.inv[v]);
+            if (meta == pack_parent(u, P::wt(e)) && t != tag_inv && t != tag_inv + 1)
+              app = atomicCAS(&g.inv[v], t, tag_inv) == t;
+          }
         }
+        warp_append(app, v, fout, fout_n, FULL);
       }
-      warp_append(app, v, fout, fout_n, FULL);
     }
+    if (lane == 0) tree[slot] = u;
   }
 }
 
@@ -1840,6 +1873,7 @@ struct FusedRepair {
 // A batch's header as the fused kernels read it.
 struct StagedBatch {
   uint64_t n, pairs, want, inv_tag;
+  unsigned long long stamp;  // C_STAMP at the kernel's start (used by its first batch)
 };
 
 // The batch crosses the bus in 16-byte loads into device scratch: the first
@@ -1849,12 +1883,13 @@ struct StagedBatch {
 // before the launch; they are read past any cache.
 constexpr unsigned APPLY_SPEC = 256;
 
-__device__ __forceinline__ void stage_batch(const ApplyHdr *hdr, const char *data, uint4 *scratch, StagedBatch &sb,
-                                            unsigned hdr_t, unsigned chunk_t) {
+__device__ __forceinline__ void stage_batch(const DevGraph &g, const ApplyHdr *hdr, const char *data, uint4 *scratch,
+                                            StagedBatch &sb, unsigned hdr_t, unsigned chunk_t) {
   const unsigned tid = threadIdx.x;
   const uint4 *raw = reinterpret_cast<const uint4 *>(data);
   if (tid >= chunk_t && tid < chunk_t + APPLY_SPEC) scratch[tid - chunk_t] = __ldcv(&raw[tid - chunk_t]);
   if (tid == hdr_t) {
+    sb.stamp = g.ctl[C_STAMP];
     sb.n = __ldcv(&hdr->n);
     sb.pairs = __ldcv(&hdr->pairs);
     sb.want = __ldcv(&hdr->want_old);
@@ -1880,7 +1915,7 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
     s_skip = second && c[C_ERR] != 0;
     if (!s_skip) {
       const unsigned long long kl = c[C_KLAUNCH];
-      prologue_ctl(c, sb.inv_tag);
+      prologue_ctl(c, sb.inv_tag, second ? nullptr : &sb.stamp);
       if (second) c[C_KLAUNCH] = kl;  // the count covers the whole submission
       c[C_CANDN] = 0;
       c[C_GROWN_OUT] = 0;
@@ -1994,7 +2029,7 @@ __global__ void __launch_bounds__(FS_TPB)
                   uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
                   cudaGraphConditionalHandle repair, FusedRepair fr, uint4 *scratch) {
   __shared__ StagedBatch sb;
-  stage_batch(hdr, data, scratch, sb, 0, 32);
+  stage_batch(g, hdr, data, scratch, sb, 0, 32);
   __syncthreads();
   const int r = apply_batch<A, W>(g, ops, sb, data, old_host, cand, add, directed, q0, mst, second, fr, scratch);
   if (threadIdx.x == 0) cudaGraphSetConditional(repair, r == 1 ? 1u : 0u);
@@ -2011,8 +2046,8 @@ __global__ void __launch_bounds__(FS_TPB)
                   const char *data2, uint32_t *cand, int directed, uint32_t *q0, uint32_t mst,
                   cudaGraphConditionalHandle left, FusedRepair fr, uint4 *scratch1, uint4 *scratch2) {
   __shared__ StagedBatch sb1, sb2;
-  stage_batch(hdr1, data1, scratch1, sb1, 0, 32);
-  stage_batch(hdr2, data2, scratch2, sb2, 32 + APPLY_SPEC, 64 + APPLY_SPEC);
+  stage_batch(g, hdr1, data1, scratch1, sb1, 0, 32);
+  stage_batch(g, hdr2, data2, scratch2, sb2, 32 + APPLY_SPEC, 64 + APPLY_SPEC);
   __syncthreads();
   int r = apply_batch<A, W>(g, ops, sb1, data1, nullptr, cand, 1, directed, q0, mst, 0, fr, scratch1);
   unsigned long long lf = r == 1 ? 1 : 0;
