@@ -184,6 +184,28 @@ int rg_level_trace(rg_graph *g, uint64_t *sizes, uint64_t cap, uint64_t *levels,
  * recorded only while rg_profile is on. */
 int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
 
+/* Device-clock stamps (ns, %globaltimer) of the last fused submission while
+ * RG_OPT_PHASE_TRACE is on: RG_PHASE_SLOTS words.  Batch b (0: the insert
+ * batch or a single batch, 1: the delete batch of rg_apply_add_del) owns
+ * words 16*b + RG_PH_*; word 16*b + 15 is 1 when that batch ran in the fused
+ * kernel.  Words 32 + 2*b and 33 + 2*b: start of the kernel that ran batch b
+ * and the end of its staging (header and edges across the bus).  The
+ * reference has no counterpart (it times phases with wall clocks). */
+#define RG_PHASE_SLOTS 64
+enum {
+  RG_PH_BEGIN = 0,      /* control block reset */
+  RG_PH_UNPACK = 1,     /* edges unpacked into the op arrays */
+  RG_PH_LOOKUP = 2,     /* edge index lookups / inserts */
+  RG_PH_GROW = 3,       /* segment growth */
+  RG_PH_WRITE = 4,      /* new slots written (insert batches) */
+  RG_PH_COUNT = 5,      /* multiplicities updated */
+  RG_PH_OLD = 6,        /* per-edge old counts and repair candidates */
+  RG_PH_SEED = 7,       /* repair seeds */
+  RG_PH_DELREPAIR = 8,  /* one-CTA deletion repair (delete batches) */
+  RG_PH_END = 9         /* in-place push levels, end of the batch */
+};
+int rg_phase_trace(rg_graph *g, uint64_t *ns);
+
 /* Strategy knobs of the level engine (the reference hard-codes its own:
  * push/pull switch at core/graph.hpp:334, vertex- vs edge-centric cost model
  * at :595-612, recompute threshold at :1252).  Values are per graph.
@@ -215,7 +237,9 @@ int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
  *   RG_OPT_FUSED_MAX      update batches of at most this many edges (0..2048,
  *                         default 2048) take the fused single-CTA path of
  *                         rg_apply_*: storage and small repairs in one
- *                         submission; larger batches run grid-wide kernels. */
+ *                         submission; larger batches run grid-wide kernels.
+ *   RG_OPT_PHASE_TRACE    1: the fused path stamps the device clock at its
+ *                         phase boundaries (rg_phase_trace); default 0. */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -228,7 +252,8 @@ typedef enum {
   RG_OPT_PULL_SPLIT = 8,
   RG_OPT_MAX_LEVELS = 9,
   RG_OPT_PULL_GROUPS = 10,
-  RG_OPT_FUSED_MAX = 11
+  RG_OPT_FUSED_MAX = 11,
+  RG_OPT_PHASE_TRACE = 12
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

@@ -120,6 +120,7 @@ def _declare(L):
         "rg_profile_read": [P, P, P],
         "rg_level_trace": [P, P, _u64, P, P],
         "rg_level_times": [P, P, _u64, P],
+        "rg_phase_trace": [P, P],
         "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
         "rg_set_option": [P, _int, _u64],
         "rg_get_option": [P, _int, P],
@@ -457,7 +458,10 @@ class Graph:
 
     OPTIONS = {"dense_pull": 0, "dense_div": 1, "lbs_min": 2, "bfs_bottom_up": 3, "recompute_min": 4, "bu_div": 5,
                "pull_div": 6, "tiny_edges": 7, "pull_split": 8, "max_levels": 9,
-               "pull_groups": 10, "fused_max": 11}
+               "pull_groups": 10, "fused_max": 11, "phase_trace": 12}
+
+    # rg_phase_trace's phase words (RG_PH_* in the header), in order
+    PHASES = ("begin", "unpack", "lookup", "grow", "write", "count", "old", "seed", "del_repair", "end")
 
     def set_option(self, name: str, value: int):
         _check(lib().rg_set_option(self._h, self.OPTIONS[name], int(value)), "rg_set_option")
@@ -474,6 +478,27 @@ class Graph:
         ms = np.zeros(int(n[0]), np.float64)
         _check(lib().rg_level_times(self._h, _p(ms), len(ms), _p(n)), "rg_level_times")
         return ms
+
+    def phase_times(self):
+        """Device time (us) of each phase of the last fused submission, per
+        batch that ran in a fused kernel: {"insert"|"delete": {phase: us}},
+        plus "staging" (header and edges across the bus) per kernel.  The
+        phase_trace option must be on; a phase a batch skipped is absent."""
+        t = np.zeros(64, np.uint64)
+        _check(lib().rg_phase_trace(self._h, _p(t)), "rg_phase_trace")
+        out = {}
+        for b, name in ((0, "insert"), (1, "delete")):
+            w = t[16 * b:16 * b + 16].astype(np.int64)
+            if w[15] != 1:
+                continue
+            d, prev = {"staging": (int(t[33 + 2 * b]) - int(t[32 + 2 * b])) / 1e3}, int(w[0])
+            for k in range(1, len(self.PHASES)):
+                if w[k] >= prev and w[k] - prev < 10**9:
+                    d[self.PHASES[k]] = (int(w[k]) - prev) / 1e3
+                    prev = int(w[k])
+            d["total"] = (prev - int(w[0])) / 1e3
+            out[name] = d
+        return out
 
     def device_bytes(self) -> int:
         b = np.zeros(1, np.uint64)

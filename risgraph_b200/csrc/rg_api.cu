@@ -255,6 +255,7 @@ int rg_destroy(rg_graph *gh) {
     if (l.exec) cudaGraphExecDestroy(l.exec);
   if (g.cap_stream) cudaStreamDestroy(g.cap_stream);
   cudaFree(g.d.trace);
+  cudaFree(g.ptrace_buf);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
   delete gh;
   return RG_OK;
@@ -541,6 +542,17 @@ int rg_level_trace(rg_graph *gh, uint64_t *sizes, uint64_t cap, uint64_t *levels
   return RG_OK;
 }
 
+int rg_phase_trace(rg_graph *gh, uint64_t *ns) {
+  if (!gh || !ns) return RG_EINVAL;
+  Graph &g = gh->g;
+  if (!g.ptrace_buf) {
+    std::memset(ns, 0, RG_PHASE_SLOTS * 8);
+    return RG_OK;
+  }
+  RG_CUDA(cudaMemcpy(ns, g.ptrace_buf, RG_PHASE_SLOTS * 8, cudaMemcpyDeviceToHost));
+  return RG_OK;
+}
+
 int rg_level_times(rg_graph *gh, double *ms, uint64_t cap, uint64_t *levels) {
   if (!gh) return RG_EINVAL;
   Graph &g = gh->g;
@@ -577,6 +589,11 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
       if (value > rg::SMALL_EDGES) break;
       g.fused_max = value;
       return RG_OK;
+    case RG_OPT_PHASE_TRACE:
+      if (value > 1) break;
+      g.phase_trace = (int)value;
+      g.d.ptrace = value ? g.ptrace_buf : nullptr;
+      return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -598,6 +615,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_MAX_LEVELS: *value = g.max_levels; return RG_OK;
     case RG_OPT_PULL_GROUPS: *value = g.pull_groups; return RG_OK;
     case RG_OPT_FUSED_MAX: *value = g.fused_max; return RG_OK;
+    case RG_OPT_PHASE_TRACE: *value = (uint64_t)g.phase_trace; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

@@ -119,6 +119,7 @@ struct DevGraph {
   uint32_t *modq;
   unsigned long long *ctl;
   unsigned long long *trace;  // frontier size per level (TRACE_CAP entries)
+  unsigned long long *ptrace; // fused-path phase stamps (RG_PHASE_SLOTS), or null when not traced
 };
 
 // ---- per-algorithm hooks (a8): update_func = better(combine(s,w), d);
@@ -203,6 +204,13 @@ __device__ __forceinline__ uint64_t ld_meta(const ulonglong2 *p) {
 __device__ __forceinline__ uint32_t ld_u32(const uint32_t *p) { return __ldcg(p); }
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// The device clock in ns (%globaltimer), for the phase trace.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Warp-aggregated append of `v` by every lane with pred set (all lanes of mask
 // must call).  Returns nothing; writes q[base + rank].
@@ -319,6 +327,8 @@ struct Graph {
   // largest batch of the fused single-CTA apply path (<= SMALL_EDGES); measured on RMAT-24
   // SSSP, larger batches run faster on the grid-wide kernels
   uint64_t fused_max = 2048;
+  int phase_trace = 0;            // RG_OPT_PHASE_TRACE
+  unsigned long long *ptrace_buf = nullptr;  // its device buffer (allocated with the labels)
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]

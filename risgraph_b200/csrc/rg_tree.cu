@@ -1910,6 +1910,11 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
   __shared__ int s_skip;
   unsigned long long *c = g.ctl;
   const unsigned tid = threadIdx.x;
+  // phase trace (RG_OPT_PHASE_TRACE): thread 0 stamps the device clock
+  unsigned long long *tr = g.ptrace ? g.ptrace + 16 * second : nullptr;
+  auto stamp = [&](int k) {
+    if (tr && tid == 0) tr[k] = global_ns();
+  };
   if (tid == 0) {
     // the second batch of a submission does nothing after an error in the first
     s_skip = second && c[C_ERR] != 0;
@@ -1924,6 +1929,8 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
   }
   __syncthreads();
   if (s_skip) return 2;
+  if (tr && tid == 0) tr[15] = 1;
+  stamp(RG_PH_BEGIN);
   const uint64_t n = sb.n < SMALL_EDGES ? sb.n : SMALL_EDGES;
   const uint64_t nops = directed ? n : 2 * n;
   const int weighted = W ? 1 : 0;
@@ -1948,8 +1955,10 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
     }
   }
   __syncthreads();
+  stamp(RG_PH_UNPACK);
   for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::lookup_op(g, ops, j, add);
   __syncthreads();
+  stamp(RG_PH_LOOKUP);
   if (add) {
     // each warp grows its own vertices (a vertex is in a grow list once); the
     // copies of long lists (a hub's) are left to the whole CTA below
@@ -1993,15 +2002,19 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
     if (tid < nbig) sdev::grow_publish(s_big_in[tid] ? g.in : g.out, s_big[tid]);
   }
   __syncthreads();
+  stamp(RG_PH_GROW);
   if (c[C_ERR]) return 2;
   if (add) {
     for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::write_new_op<W>(g, ops, j);
     __syncthreads();
+    stamp(RG_PH_WRITE);
   }
   for (uint64_t j = tid; j < nops; j += FS_TPB) sdev::count_op<W>(g, ops, j, add);
   __syncthreads();
+  stamp(RG_PH_COUNT);
   for (uint64_t i = tid; i < n; i += FS_TPB) sdev::edge_old(ops, i, directed, add, 1, sb.want ? old_host : nullptr, cand, c);
   __syncthreads();
+  stamp(RG_PH_OLD);
   const uint64_t ncand = c[C_CANDN];
   const uint64_t warp = tid >> 5, nwarps = FS_TPB / 32;
   if (add) {
@@ -2011,14 +2024,17 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
     seed_del(g, ops.src, ops.dst, ops.w, cand, ncand, directed, q0, &c[C_QN0], warp, nwarps);
   }
   __syncthreads();
+  stamp(RG_PH_SEED);
   bool over = false;
   if (c[C_QN0] && !c[C_ERR]) {
     if (!add) over = del_tiny_levels<A, W>(g, q0, fr.q1, fr.tree, fr.limit, fr.big, fr.max_iter, mst);
+    stamp(RG_PH_DELREPAIR);
     if (!over && fr.tiny_edges && c[C_QN0])
       tiny_levels<A, W>(g, q0, &c[C_QN0], fr.q1, &c[C_QN1], q0, &c[C_QN0], fr.max_levels, fr.tiny_edges, mst, false);
   }
   const bool left = over || (c[C_QN0] && !c[C_ERR]);
   __syncthreads();  // every thread has read the counts before the next batch resets them
+  stamp(RG_PH_END);
   if (tid == 0) c[C_OVER] = over ? 1 : 0;
   return left ? 1 : 0;
 }
@@ -2029,8 +2045,14 @@ __global__ void __launch_bounds__(FS_TPB)
                   uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
                   cudaGraphConditionalHandle repair, FusedRepair fr, uint4 *scratch) {
   __shared__ StagedBatch sb;
+  if (g.ptrace && threadIdx.x == 0) {
+    g.ptrace[32 + 2 * second] = global_ns();
+    g.ptrace[16 * second + 15] = 0;
+    if (!second) g.ptrace[31] = 0;  // a single batch: no delete batch ran
+  }
   stage_batch(g, hdr, data, scratch, sb, 0, 32);
   __syncthreads();
+  if (g.ptrace && threadIdx.x == 0) g.ptrace[33 + 2 * second] = global_ns();
   const int r = apply_batch<A, W>(g, ops, sb, data, old_host, cand, add, directed, q0, mst, second, fr, scratch);
   if (threadIdx.x == 0) cudaGraphSetConditional(repair, r == 1 ? 1u : 0u);
 }
@@ -2046,9 +2068,14 @@ __global__ void __launch_bounds__(FS_TPB)
                   const char *data2, uint32_t *cand, int directed, uint32_t *q0, uint32_t mst,
                   cudaGraphConditionalHandle left, FusedRepair fr, uint4 *scratch1, uint4 *scratch2) {
   __shared__ StagedBatch sb1, sb2;
+  if (g.ptrace && threadIdx.x == 0) {
+    g.ptrace[32] = g.ptrace[34] = global_ns();
+    g.ptrace[15] = g.ptrace[31] = 0;
+  }
   stage_batch(g, hdr1, data1, scratch1, sb1, 0, 32);
   stage_batch(g, hdr2, data2, scratch2, sb2, 32 + APPLY_SPEC, 64 + APPLY_SPEC);
   __syncthreads();
+  if (g.ptrace && threadIdx.x == 0) g.ptrace[33] = g.ptrace[35] = global_ns();
   int r = apply_batch<A, W>(g, ops, sb1, data1, nullptr, cand, 1, directed, q0, mst, 0, fr, scratch1);
   unsigned long long lf = r == 1 ? 1 : 0;
   if (r == 0) {
@@ -2880,6 +2907,9 @@ int tree_alloc(Graph &g) {
     RG_CUDA(cudaMemcpy(&g.d.ctl[C_MODEPOCH], &one, 8, cudaMemcpyHostToDevice));
   }
   if ((rc = alloc((void **)&g.d.trace, TRACE_CAP * 8, "level trace"))) return rc;
+  if ((rc = alloc((void **)&g.ptrace_buf, RG_PHASE_SLOTS * 8, "phase trace"))) return rc;
+  RG_CUDA(cudaMemset(g.ptrace_buf, 0, RG_PHASE_SLOTS * 8));
+  g.d.ptrace = g.phase_trace ? g.ptrace_buf : nullptr;
   RG_CUDA(cudaMemset(g.d.stamp, 0, V * 4 + 4));
   RG_CUDA(cudaMemset(g.d.inv, 0, V * 4 + 4));
   RG_CUDA(cudaMemset(g.d.chk, 0, V * 4 + 4));
@@ -2989,6 +3019,7 @@ int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, si
 
 uint64_t apply_key(const Graph &g, const LevelCfg &cfg) {
   return splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
+         splitmix64((uint64_t)(uintptr_t)g.d.ptrace + 17) ^
          splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^ splitmix64((uint64_t)(uintptr_t)g.stage_dev + 13) ^
          cfg_key(cfg) ^ splitmix64(recompute_threshold(g) + 11);
 }
