@@ -218,8 +218,10 @@ int rg_create(uint64_t vertices, uint64_t hint_edges, int symmetric, int dual, i
   g.stream = g.own_stream;
   if (!rc && (e = cudaEventCreate(&g.pev[0])) != cudaSuccess) rc = rg::cuda_fail(e, "event");
   if (!rc && (e = cudaEventCreate(&g.pev[1])) != cudaSuccess) rc = rg::cuda_fail(e, "event");
-  if (!rc && (e = cudaHostAlloc(&g.h_ctl, sizeof(unsigned long long) * rg::C_COUNT, cudaHostAllocDefault)) != cudaSuccess)
+  if (!rc && (e = cudaHostAlloc(&g.h_ctl, sizeof(unsigned long long) * rg::C_COUNT, cudaHostAllocMapped)) != cudaSuccess)
     rc = rg::cuda_fail(e, "cudaHostAlloc(ctl)");
+  if (!rc && (e = cudaHostGetDevicePointer(&g.h_ctl_dev, g.h_ctl, 0)) != cudaSuccess)
+    rc = rg::cuda_fail(e, "cudaHostGetDevicePointer(ctl)");
   if (!rc) rc = rg::storage_alloc(g);
   if (!rc) rc = rg::tree_alloc(g);
   if (rc) {
@@ -252,6 +254,8 @@ int rg_destroy(rg_graph *gh) {
   for (auto &l : g.applies)
     if (l.exec) cudaGraphExecDestroy(l.exec);
   for (auto &l : g.mixes)
+    if (l.exec) cudaGraphExecDestroy(l.exec);
+  for (auto &l : g.rests)
     if (l.exec) cudaGraphExecDestroy(l.exec);
   if (g.cap_stream) cudaStreamDestroy(g.cap_stream);
   cudaFree(g.d.trace);

@@ -71,7 +71,7 @@ enum Ctl : int {
   C_HVE = 28,      // ... by the expand pass
   C_HVP = 29,      // ... by the pull over the reset set
   C_OVER = 30,     // the fused apply's one-CTA deletion repair handed over to the grid-wide one
-  C_LEFT = 31,     // what the insert+delete kernel left to the graph (1: insert loop and delete batch, 2: delete repair)
+  C_LEFT = 31,     // what a fused kernel left to the host (1: insert batch's level loop [and the delete batch], 2: delete batch's repair)
   C_COUNT = 32
 };
 
@@ -283,7 +283,8 @@ struct Graph {
   size_t stage_host_bytes = 0;
   uint32_t *ops = nullptr;     // s,d,w,rid,old... per directed op (SoA inside)
   uint64_t ops_cap = 0;
-  unsigned long long *h_ctl = nullptr;  // pinned mirror of ctl
+  unsigned long long *h_ctl = nullptr;      // pinned, mapped mirror of ctl
+  unsigned long long *h_ctl_dev = nullptr;  // its device view (the fused kernels write it)
   uint32_t stamp_epoch = 0;
   uint32_t inv_epoch = 0;
   uint32_t mod_epoch = 1;
@@ -333,7 +334,8 @@ struct Graph {
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays
   // device-driven level loops: [algo][weighted][build variant]; deletion repair: [algo][weighted]
   LoopGraph loops[16];
-  LoopGraph dels[8];
+  LoopGraph dels[16];
+  LoopGraph rests[16];  // after an insert+delete kernel left the insert batch's loop: loop -> delete batch
   // fused small-batch apply graphs: [algo][weighted][add][directed]; insert+delete pairs: [algo][weighted][directed]
   LoopGraph applies[32];
   LoopGraph mixes[16];

@@ -1850,11 +1850,13 @@ __global__ void k_handover(DevGraph g, cudaGraphConditionalHandle standard) {
 // the tree repair, with CTA barriers where the multi-kernel path has kernel
 // boundaries.  A small repair then runs in the same CTA: the one-CTA deletion
 // repair (del_tiny_levels) for a delete batch, and push levels while the
-// frontier stays small (tiny_levels).  Only what is left opens the conditional
-// node after the kernel (`repair`), whose body runs the grid-wide deletion
-// repair when the one-CTA repair handed over (C_OVER) and the level loop.  A
-// safe update (the common case, need_update_tree_* false) and most unsafe
-// single updates cost this one kernel.  A storage error (edge
+// frontier stays small (tiny_levels).  The kernel ends by writing the control
+// block to the host's mapped copy; C_LEFT there tells the host what is left
+// for the graphs it launches next (the level loop; the grid-wide deletion
+// repair when the one-CTA repair handed over, C_OVER).  A safe update (the
+// common case, need_update_tree_* false) and most unsafe single updates cost
+// this one kernel and no conditional node: a conditional node costs about
+// 10 us even when its condition is false.  A storage error (edge
 // index or pool full) stops before the count step, leaving the op arrays for
 // the host's compaction and replay, exactly like the multi-kernel path.
 constexpr int FS_TPB = 1024;
@@ -1869,6 +1871,14 @@ struct FusedRepair {
   uint64_t max_levels;  // level bound of the push loop
   uint64_t tiny_edges;  // out-slot limit of an in-place push level (0: none in place)
 };
+
+// The control block to the host's mapped copy, by the whole CTA after its
+// last update (the host reads it once the stream has synchronised).
+__device__ __forceinline__ void ctl_to_host(const DevGraph &g, unsigned long long *ctl_host) {
+  __syncthreads();
+  if (threadIdx.x < C_COUNT) ctl_host[threadIdx.x] = g.ctl[threadIdx.x];
+  __threadfence_system();
+}
 
 // A batch's header as the fused kernels read it.
 struct StagedBatch {
@@ -2042,8 +2052,8 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
 template <int A, bool W>
 __global__ void __launch_bounds__(FS_TPB)
     k_apply_small(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr, const char *data, uint64_t *old_host,
-                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second,
-                  cudaGraphConditionalHandle repair, FusedRepair fr, uint4 *scratch) {
+                  uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, int second, FusedRepair fr,
+                  uint4 *scratch, unsigned long long *ctl_host) {
   __shared__ StagedBatch sb;
   if (g.ptrace && threadIdx.x == 0) {
     g.ptrace[32 + 2 * second] = global_ns();
@@ -2054,19 +2064,20 @@ __global__ void __launch_bounds__(FS_TPB)
   __syncthreads();
   if (g.ptrace && threadIdx.x == 0) g.ptrace[33 + 2 * second] = global_ns();
   const int r = apply_batch<A, W>(g, ops, sb, data, old_host, cand, add, directed, q0, mst, second, fr, scratch);
-  if (threadIdx.x == 0) cudaGraphSetConditional(repair, r == 1 ? 1u : 0u);
+  if (threadIdx.x == 0) g.ctl[C_LEFT] = r == 1 ? (add ? 1 : 2) : 0;
+  ctl_to_host(g, ctl_host);
 }
 
 // An insert batch and then a delete batch in one kernel (both staged in one
 // round trip): the delete batch runs here too when the insert batch's repair
-// finished in place.  C_LEFT tells the IF body after the kernel what is left:
-// 1 the insert batch's level loop and then the whole delete batch, 2 the
-// delete batch's repair.
+// finished in place.  C_LEFT tells the host what is left: 1 the insert
+// batch's level loop and then the whole delete batch, 2 the delete batch's
+// repair.
 template <int A, bool W>
 __global__ void __launch_bounds__(FS_TPB)
     k_apply_mixed(DevGraph g, sdev::OpView ops, const ApplyHdr *hdr1, const char *data1, const ApplyHdr *hdr2,
-                  const char *data2, uint32_t *cand, int directed, uint32_t *q0, uint32_t mst,
-                  cudaGraphConditionalHandle left, FusedRepair fr, uint4 *scratch1, uint4 *scratch2) {
+                  const char *data2, uint32_t *cand, int directed, uint32_t *q0, uint32_t mst, FusedRepair fr,
+                  uint4 *scratch1, uint4 *scratch2, unsigned long long *ctl_host) {
   __shared__ StagedBatch sb1, sb2;
   if (g.ptrace && threadIdx.x == 0) {
     g.ptrace[32] = g.ptrace[34] = global_ns();
@@ -2082,17 +2093,8 @@ __global__ void __launch_bounds__(FS_TPB)
     r = apply_batch<A, W>(g, ops, sb2, data2, nullptr, cand, 0, directed, q0, mst, 1, fr, scratch2);
     lf = r == 1 ? 2 : 0;
   }
-  if (threadIdx.x == 0) {
-    g.ctl[C_LEFT] = lf;
-    cudaGraphSetConditional(left, lf ? 1u : 0u);
-  }
-}
-
-// Selects the SWITCH case of the IF body after k_apply_mixed.
-__global__ void k_left(DevGraph g, cudaGraphConditionalHandle sw) {
-  const unsigned long long lf = g.ctl[C_LEFT];
-  g.ctl[C_KLAUNCH] += lf == 1 ? 2 : 1;  // this kernel, and the delete batch's own kernel in case 1
-  cudaGraphSetConditional(sw, (unsigned)lf);
+  if (threadIdx.x == 0) g.ctl[C_LEFT] = lf;
+  ctl_to_host(g, ctl_host);
 }
 
 // need_update_tree_add (core/graph.hpp:987-1000) / need_update_tree_del
@@ -2678,8 +2680,8 @@ int push_levels(Graph &g, bool build_variant) {
 
 // Cached standalone deletion repair (the push loop follows as its own graph).
 template <int A, bool W>
-int del_exec(Graph &g, cudaGraphExec_t *out) {
-  LoopGraph &slot = g.dels[A * 2 + (W ? 1 : 0)];
+int del_exec(Graph &g, bool fused, cudaGraphExec_t *out) {
+  LoopGraph &slot = g.dels[(A * 2 + (W ? 1 : 0)) * 2 + (fused ? 1 : 0)];
   const uint64_t key = (g.layout_version << 40) ^ recompute_threshold(g);
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
@@ -2692,7 +2694,7 @@ int del_exec(Graph &g, cudaGraphExec_t *out) {
   cudaGraph_t graph;
   RG_CUDA(cudaGraphCreate(&graph, 0));
   cudaGraphNode_t last;
-  int rc = add_del_repair<A, W>(g, graph, nullptr, 0, &last);
+  int rc = add_del_repair<A, W>(g, graph, nullptr, 0, &last, fused);
   if (!rc) {
     cudaError_t e = cudaGraphInstantiate(&slot.exec, graph, 0);
     if (e != cudaSuccess) {
@@ -2798,7 +2800,7 @@ int del_enqueue(Graph &g, uint64_t n_edges, int directed, bool from_cands) {
     rc = del_repair_stepped<A, W>(g);
   } else {
     cudaGraphExec_t exec;
-    if ((rc = del_exec<A, W>(g, &exec))) return rc;
+    if ((rc = del_exec<A, W>(g, false, &exec))) return rc;
     RG_CUDA(cudaGraphLaunch(exec, g.stream));
   }
   if (rc) return rc;
@@ -2972,14 +2974,12 @@ FusedRepair fused_repair(const Graph &g, const LevelCfg &cfg) {
   return fr;
 }
 
-// One fused apply phase as graph nodes: k_apply_small (reading the header at
-// hdr_off of the staging buffer; it runs small repairs itself) -> IF (work is
-// left) { [k_handover -> IF (its deletion repair handed over) { grid-wide
-// deletion repair } ->] level loop }.  *out is the IF node.
+// The fused kernel for one batch as a graph node after `deps`: k_apply_small
+// with the header at hdr_off of the staging buffer (second: the delete batch
+// of an insert+delete submission, whose edges start at apply_data2_off()).
 template <int A, bool W>
-int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps,
-                    cudaGraphConditionalHandle ih, bool add, int directed, uint64_t hdr_off, int second,
-                    const LevelCfg &cfg, cudaGraphNode_t *out) {
+int add_apply_kernel(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps, bool add, int directed,
+                     uint64_t hdr_off, int second, const LevelCfg &cfg, cudaGraphNode_t *out) {
   sdev::OpView ops = sdev::op_view(g);
   char *base = reinterpret_cast<char *>(g.stage_host_dev);
   const ApplyHdr *hdr = reinterpret_cast<const ApplyHdr *>(base + hdr_off);
@@ -2991,49 +2991,29 @@ int add_apply_phase(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, si
   uint32_t *q0 = g.q[0];
   uint32_t mst = mod_stamp(g);
   FusedRepair fr = fused_repair(g, cfg);
-  cudaError_t e = cudaSuccess;
-  void *args[] = {(void *)&g.d,  (void *)&ops, (void *)&hdr, (void *)&data,     (void *)&old_host, (void *)&cand,
-                  (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst, (void *)&a_second, (void *)&ih,
-                  (void *)&fr,   (void *)&scratch};
+  unsigned long long *ctl_host = g.h_ctl_dev;
+  void *args[] = {(void *)&g.d,    (void *)&ops, (void *)&hdr, (void *)&data,   (void *)&old_host,
+                  (void *)&cand,   (void *)&a_add, (void *)&a_dir, (void *)&q0, (void *)&mst,
+                  (void *)&a_second, (void *)&fr, (void *)&scratch, (void *)&ctl_host};
   cudaKernelNodeParams kp = {};
   kp.func = (void *)k_apply_small<A, W>;
   kp.gridDim = dim3(1);
   kp.blockDim = dim3(FS_TPB);
   kp.kernelParams = args;
-  cudaGraphNode_t kn;
-  if ((e = cudaGraphAddKernelNode(&kn, graph, deps, ndeps, &kp)) != cudaSuccess)
-    return cuda_fail(e, "building the fused apply graph");
-  cudaGraphNodeParams ip = {};
-  ip.type = cudaGraphNodeTypeConditional;
-  ip.conditional.handle = ih;
-  ip.conditional.type = cudaGraphCondTypeIf;
-  ip.conditional.size = 1;
-  if ((e = cudaGraphAddNode(out, graph, &kn, 1, &ip)) != cudaSuccess) return cuda_fail(e, "building the fused apply graph");
-  cudaGraph_t body = ip.conditional.phGraph_out[0];
-  cudaGraphNode_t last, loop;
-  if (add) return add_level_loop<A, W>(g, body, nullptr, 0, cfg, &loop);
-  int rc = add_del_repair<A, W>(g, body, nullptr, 0, &last, true);
-  if (!rc) rc = add_level_loop<A, W>(g, body, &last, 1, cfg, &loop);
-  return rc;
+  cudaError_t e = cudaGraphAddKernelNode(out, graph, deps, ndeps, &kp);
+  return e == cudaSuccess ? RG_OK : cuda_fail(e, "building the fused apply graph");
 }
 
 uint64_t apply_key(const Graph &g, const LevelCfg &cfg) {
   return splitmix64(g.layout_version) ^ splitmix64((uint64_t)(uintptr_t)g.ops ^ (g.ops_cap << 1)) ^
-         splitmix64((uint64_t)(uintptr_t)g.d.ptrace + 17) ^
+         splitmix64((uint64_t)(uintptr_t)g.d.ptrace + 17) ^ splitmix64((uint64_t)(uintptr_t)g.h_ctl_dev + 19) ^
          splitmix64((uint64_t)(uintptr_t)g.stage_host_dev + 7) ^ splitmix64((uint64_t)(uintptr_t)g.stage_dev + 13) ^
          cfg_key(cfg) ^ splitmix64(recompute_threshold(g) + 11);
 }
 
-// Insert batch then delete batch in one graph: k_apply_mixed (both batches,
-// and their repairs while they stay small) -> IF (work is left) { k_left ->
-// SWITCH { 1: level loop -> the delete batch's phase (add_apply_phase, skipped
-// after an error in the insert batch) | 2: the rest of the delete batch's
-// repair } } -> control block to the host.
-template <int A, bool W>
-int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
-  LoopGraph &slot = g.mixes[(A * 2 + (W ? 1 : 0)) * 2 + (directed ? 1 : 0)];
-  const LevelCfg cfg = level_cfg(g, A, false);
-  const uint64_t key = apply_key(g, cfg);
+// A cached graph: `build` adds its nodes; rebuilt when `key` changes.
+template <typename F>
+int cached_graph(LoopGraph &slot, uint64_t key, F build, const char *what, cudaGraphExec_t *out) {
   if (slot.exec && slot.key == key) {
     *out = slot.exec;
     return RG_OK;
@@ -3044,15 +3024,31 @@ int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
   }
   cudaGraph_t graph;
   RG_CUDA(cudaGraphCreate(&graph, 0));
-  int rc = RG_OK;
-  cudaError_t e = cudaSuccess;
-  do {
-    cudaGraphConditionalHandle hl;
-    if ((e = cudaGraphConditionalHandleCreate(&hl, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
+  int rc = build(graph);
+  if (!rc) {
+    cudaError_t e = cudaGraphInstantiate(&slot.exec, graph, 0);
+    if (e != cudaSuccess) {
+      slot.exec = nullptr;
+      rc = cuda_fail(e, what);
+    }
+  }
+  cudaGraphDestroy(graph);
+  if (rc) return rc;
+  slot.key = key;
+  *out = slot.exec;
+  return RG_OK;
+}
+
+// Insert batch then delete batch: one node, k_apply_mixed (both batches, and
+// their repairs while they stay small).
+template <int A, bool W>
+int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
+  const LevelCfg cfg = level_cfg(g, A, false);
+  auto build = [&](cudaGraph_t graph) -> int {
     sdev::OpView ops = sdev::op_view(g);
     char *base = reinterpret_cast<char *>(g.stage_host_dev);
-    const ApplyHdr *hdr1 = reinterpret_cast<const ApplyHdr *>(base), *hdr2 =
-                                                                         reinterpret_cast<const ApplyHdr *>(base + APPLY_HDR2);
+    const ApplyHdr *hdr1 = reinterpret_cast<const ApplyHdr *>(base);
+    const ApplyHdr *hdr2 = reinterpret_cast<const ApplyHdr *>(base + APPLY_HDR2);
     const char *data1 = base + APPLY_DATA_OFF, *data2 = base + APPLY_DATA_OFF + apply_data2_off();
     uint4 *scr1 = reinterpret_cast<uint4 *>(g.stage_dev);
     uint4 *scr2 = reinterpret_cast<uint4 *>(reinterpret_cast<char *>(g.stage_dev) + apply_data2_off());
@@ -3060,116 +3056,68 @@ int mixed_exec(Graph &g, int directed, cudaGraphExec_t *out) {
     int a_dir = directed ? 1 : 0;
     uint32_t mst = mod_stamp(g);
     FusedRepair fr = fused_repair(g, cfg);
-    void *args[] = {(void *)&g.d,   (void *)&ops, (void *)&hdr1, (void *)&data1, (void *)&hdr2, (void *)&data2,
-                    (void *)&cand,  (void *)&a_dir, (void *)&q0, (void *)&mst,   (void *)&hl,   (void *)&fr,
-                    (void *)&scr1, (void *)&scr2};
+    unsigned long long *ctl_host = g.h_ctl_dev;
+    void *args[] = {(void *)&g.d,  (void *)&ops,   (void *)&hdr1, (void *)&data1, (void *)&hdr2,
+                    (void *)&data2, (void *)&cand, (void *)&a_dir, (void *)&q0,   (void *)&mst,
+                    (void *)&fr,   (void *)&scr1,  (void *)&scr2, (void *)&ctl_host};
     cudaKernelNodeParams kp = {};
     kp.func = (void *)k_apply_mixed<A, W>;
     kp.gridDim = dim3(1);
     kp.blockDim = dim3(FS_TPB);
     kp.kernelParams = args;
     cudaGraphNode_t kn;
-    if ((e = cudaGraphAddKernelNode(&kn, graph, nullptr, 0, &kp)) != cudaSuccess) break;
-    cudaGraphNodeParams ip = {};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = hl;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    cudaGraphNode_t ifn;
-    if ((e = cudaGraphAddNode(&ifn, graph, &kn, 1, &ip)) != cudaSuccess) break;
-    cudaGraph_t body = ip.conditional.phGraph_out[0];
-    cudaGraphConditionalHandle sw;
-    if ((e = cudaGraphConditionalHandleCreate(&sw, body, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    void *la[] = {(void *)&g.d, (void *)&sw};
-    cudaKernelNodeParams lp = {};
-    lp.func = (void *)k_left;
-    lp.gridDim = dim3(1);
-    lp.blockDim = dim3(1);
-    lp.kernelParams = la;
-    cudaGraphNode_t ln;
-    if ((e = cudaGraphAddKernelNode(&ln, body, nullptr, 0, &lp)) != cudaSuccess) break;
-    cudaGraphNodeParams sp = {};
-    sp.type = cudaGraphNodeTypeConditional;
-    sp.conditional.handle = sw;
-    sp.conditional.type = cudaGraphCondTypeSwitch;
-    sp.conditional.size = 3;
-    cudaGraphNode_t sn;
-    if ((e = cudaGraphAddNode(&sn, body, &ln, 1, &sp)) != cudaSuccess) break;
-    // case 1: the insert batch's level loop, then the delete batch as its own phase
-    cudaGraph_t c1 = sp.conditional.phGraph_out[1];
-    cudaGraphNode_t loop1, ph2;
-    if ((rc = add_level_loop<A, W>(g, c1, nullptr, 0, cfg, &loop1))) break;
-    cudaGraphConditionalHandle h3;
-    if ((e = cudaGraphConditionalHandleCreate(&h3, c1, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    if ((rc = add_apply_phase<A, W>(g, c1, &loop1, 1, h3, false, directed, APPLY_HDR2, 1, cfg, &ph2))) break;
-    // case 2: the rest of the delete batch's repair
-    cudaGraph_t c2 = sp.conditional.phGraph_out[2];
-    cudaGraphNode_t rep2, loop2;
-    if ((rc = add_del_repair<A, W>(g, c2, nullptr, 0, &rep2, true))) break;
-    if ((rc = add_level_loop<A, W>(g, c2, &rep2, 1, cfg, &loop2))) break;
-    cudaGraphNode_t mn;
-    if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &ifn, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
-                                      cudaMemcpyDeviceToHost)) != cudaSuccess)
-      break;
-    e = cudaGraphInstantiate(&slot.exec, graph, 0);
-  } while (0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
-    slot.exec = nullptr;
-    return cuda_fail(e, "building the fused insert+delete graph");
-  }
-  if (rc) {
-    slot.exec = nullptr;
-    return rc;
-  }
-  slot.key = key;
-  *out = slot.exec;
-  return RG_OK;
+    cudaError_t e = cudaGraphAddKernelNode(&kn, graph, nullptr, 0, &kp);
+    return e == cudaSuccess ? RG_OK : cuda_fail(e, "building the fused insert+delete graph");
+  };
+  return cached_graph(g.mixes[(A * 2 + (W ? 1 : 0)) * 2 + (directed ? 1 : 0)], apply_key(g, cfg), build,
+                      "instantiating the fused insert+delete graph", out);
 }
 
-// Fused small-batch apply graph per (algorithm, weighting, add/delete,
-// directed): the nodes of add_apply_phase -> control block to the host.  Its parameters hold the op, staging and pool
-// addresses, so it is rebuilt when any of them moves.
+// After k_apply_mixed left the insert batch's level loop: that loop, then the
+// delete batch in its own fused kernel (k_apply_small, second batch).
+template <int A, bool W>
+int rest_exec(Graph &g, int directed, cudaGraphExec_t *out) {
+  const LevelCfg cfg = level_cfg(g, A, false);
+  auto build = [&](cudaGraph_t graph) -> int {
+    cudaGraphNode_t loop, kn;
+    int rc = add_level_loop<A, W>(g, graph, nullptr, 0, cfg, &loop);
+    if (!rc) rc = add_apply_kernel<A, W>(g, graph, &loop, 1, false, directed, APPLY_HDR2, 1, cfg, &kn);
+    return rc;
+  };
+  return cached_graph(g.rests[(A * 2 + (W ? 1 : 0)) * 2 + (directed ? 1 : 0)], apply_key(g, cfg), build,
+                      "instantiating the insert loop + delete batch graph", out);
+}
+
+// One batch: one node, k_apply_small.  Its parameters hold the op, staging and
+// pool addresses, so it is rebuilt when any of them moves.
 template <int A, bool W>
 int apply_exec(Graph &g, bool add, int directed, cudaGraphExec_t *out) {
-  LoopGraph &slot = g.applies[((A * 2 + (W ? 1 : 0)) * 2 + (add ? 1 : 0)) * 2 + (directed ? 1 : 0)];
   const LevelCfg cfg = level_cfg(g, A, false);
-  const uint64_t key = apply_key(g, cfg);
-  if (slot.exec && slot.key == key) {
-    *out = slot.exec;
-    return RG_OK;
-  }
-  if (slot.exec) {
-    cudaGraphExecDestroy(slot.exec);
-    slot.exec = nullptr;
-  }
-  cudaGraph_t graph;
-  RG_CUDA(cudaGraphCreate(&graph, 0));
+  auto build = [&](cudaGraph_t graph) -> int {
+    cudaGraphNode_t kn;
+    return add_apply_kernel<A, W>(g, graph, nullptr, 0, add, directed, 0, 0, cfg, &kn);
+  };
+  return cached_graph(g.applies[((A * 2 + (W ? 1 : 0)) * 2 + (add ? 1 : 0)) * 2 + (directed ? 1 : 0)],
+                      apply_key(g, cfg), build, "instantiating the fused apply graph", out);
+}
+
+// What a fused kernel left (C_LEFT in the host's copy of the control block):
+// 1 the insert batch's level loop; 2 the delete batch's repair, that is the
+// grid-wide deletion repair when the one-CTA repair handed over (k_handover
+// reads C_OVER) and then the level loop.  Ends with the control block read
+// back.
+template <int A, bool W>
+int finish_left(Graph &g, unsigned long long left) {
   int rc = RG_OK;
-  cudaError_t e = cudaSuccess;
-  do {
-    cudaGraphConditionalHandle ih;
-    if ((e = cudaGraphConditionalHandleCreate(&ih, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) break;
-    cudaGraphNode_t ifn;
-    if ((rc = add_apply_phase<A, W>(g, graph, nullptr, 0, ih, add, directed, 0, 0, cfg, &ifn))) break;
-    cudaGraphNode_t mn;
-    if ((e = cudaGraphAddMemcpyNode1D(&mn, graph, &ifn, 1, g.h_ctl, g.d.ctl, sizeof(unsigned long long) * C_COUNT,
-                                      cudaMemcpyDeviceToHost)) != cudaSuccess)
-      break;
-    e = cudaGraphInstantiate(&slot.exec, graph, 0);
-  } while (0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
-    slot.exec = nullptr;
-    return cuda_fail(e, "building the fused apply graph");
+  if (left == 2) {
+    cudaGraphExec_t de;
+    if ((rc = del_exec<A, W>(g, true, &de))) return rc;
+    RG_CUDA(cudaGraphLaunch(de, g.stream));
   }
-  if (rc) {
-    slot.exec = nullptr;
-    return rc;
-  }
-  slot.key = key;
-  *out = slot.exec;
-  return RG_OK;
+  cudaGraphExec_t le;
+  if ((rc = loop_exec<A, W>(g, false, &le))) return rc;
+  RG_CUDA(cudaGraphLaunch(le, g.stream));
+  return read_ctl(g);
 }
 
 template <int A, bool W>
@@ -3216,6 +3164,7 @@ int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_
     replayed = true;
   }
   if ((rc = storage_error(g))) return rc;
+  if (!replayed && g.h_ctl[C_LEFT] && (rc = finish_left<A, W>(g, g.h_ctl[C_LEFT]))) return rc;
   if ((rc = after_sync<A, W>(g, what))) return rc;
   if (old_num) std::memcpy(old_num, replayed ? (const void *)storage_old_host(g) : (const void *)(st + apply_old_off()),
                            n * 8);
@@ -3261,6 +3210,18 @@ int apply_add_del_t(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge
     return n_del ? apply_small_t<A, W>(g, dels, nullptr, n_del, directed, false, nullptr) : RG_OK;
   }
   if ((rc = storage_error(g))) return rc;
+  unsigned long long left = g.h_ctl[C_LEFT];
+  if (left == 1) {
+    // the insert batch's level loop, then the delete batch in its own kernel
+    cudaGraphExec_t re;
+    if ((rc = rest_exec<A, W>(g, directed, &re))) return rc;
+    count_launch(g);
+    RG_CUDA(cudaGraphLaunch(re, g.stream));
+    RG_CUDA(cudaStreamSynchronize(g.stream));
+    if ((rc = storage_error(g))) return rc;
+    left = g.h_ctl[C_LEFT];
+  }
+  if (left == 2 && (rc = finish_left<A, W>(g, 2))) return rc;
   return after_sync<A, W>(g, 2);
 }
 
