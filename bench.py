@@ -403,12 +403,14 @@ def leg_served(args):
     import risgraph_b200 as rg
     from risgraph_b200 import gen
     scale = args.served_scale
-    pairs = gen.rmat(scale, seed=args.seed)
     V = 1 << scale
-    E = len(pairs)
+    E = 16 * V
     imported = int(E * 0.9)
-    root = gen.max_out_degree_vertex(pairs, V)
-    g = rg.Graph(V, E, weighted=True)
+    # the update stream continues past the graph's 16 * 2^scale edges (the same
+    # counter-based generator), so that the fastest load cannot exhaust it
+    pairs = gen.rmat(scale, n_edges=E + E // 4, seed=args.seed)
+    root = gen.max_out_degree_vertex(pairs[:E], V)
+    g = rg.Graph(V, len(pairs), weighted=True)
     g.add_pairs(pairs[:imported], True, want_old=False)
     g.build_tree("sssp", root)
     offset = 0
@@ -474,6 +476,7 @@ def leg_served(args):
 
 
 MIX = [(24, "sssp"), (23, "bfs"), (22, "wcc"), (20, "sssp"), (18, "bfs"), (16, "wcc")]
+MIX_STREAM_MIN = 4 << 20   # update-stream edges past the loaded ones, per instance
 
 
 def leg_served_mix(args):
@@ -490,10 +493,12 @@ def leg_served_mix(args):
     from risgraph_b200 import gen
     insts = []
     for scale, algo in MIX:
-        pairs = gen.rmat(scale, seed=scale)
         V = 1 << scale
-        imported = int(len(pairs) * 0.9)
-        root = gen.max_out_degree_vertex(pairs, V)
+        imported = int(16 * V * 0.9)
+        # each instance's update stream continues past its 16 * 2^scale edges, so
+        # that the small instances keep their share of the load at every point
+        pairs = gen.rmat(scale, n_edges=max(16 * V, imported + MIX_STREAM_MIN), seed=scale)
+        root = gen.max_out_degree_vertex(pairs[:16 * V], V)
         g = rg.Graph(V, len(pairs), symmetric=algo == "wcc", dual=algo != "wcc", weighted=algo == "sssp")
         g.add_pairs(pairs[:imported], algo != "wcc", want_old=False)
         g.build_tree(algo, root)
@@ -540,7 +545,7 @@ def leg_served_mix(args):
                     break
                 if per_update and best is not None and len(sweep) > 1 and sweep[-2]["p99_us"] > 1000.0:
                     break                # came down to a sustainable load
-                total *= 2
+                total = total * 2 if total < 2048 else total * 3 // 2   # finer steps near the knee
             for k in ids:
                 srv.detach(k)
         out[mode] = {"best_at_p99_le_1ms": best, "sweep": sweep}

@@ -183,6 +183,12 @@ int rg_level_trace(rg_graph *g, uint64_t *sizes, uint64_t cap, uint64_t *levels,
 /* Device time (ms, CUDA events) of each push level of the last tree call,
  * recorded only while rg_profile is on. */
 int rg_level_times(rg_graph *g, double *ms, uint64_t cap, uint64_t *levels);
+/* Device-clock start (ns, %globaltimer) of each level of the last tree call,
+ * stamped on the device by the level loop itself, so it covers graph-launched
+ * calls too; entry `levels` is the end of the last level.  Writes
+ * min(cap, levels + 1) entries.  No counterpart in the reference (it times
+ * whole calls with wall clocks, src/sssp.cpp:96-99). */
+int rg_level_stamps(rg_graph *g, uint64_t *ns, uint64_t cap, uint64_t *levels);
 
 /* Device-clock stamps (ns, %globaltimer) of the last fused submission while
  * RG_OPT_PHASE_TRACE is on: RG_PHASE_SLOTS words.  Batch b (0: the insert
@@ -239,7 +245,11 @@ int rg_phase_trace(rg_graph *g, uint64_t *ns);
  *                         rg_apply_*: storage and small repairs in one
  *                         submission; larger batches run grid-wide kernels.
  *   RG_OPT_PHASE_TRACE    1: the fused path stamps the device clock at its
- *                         phase boundaries (rg_phase_trace); default 0. */
+ *                         phase boundaries (rg_phase_trace); default 0.
+ *   RG_OPT_INLINE_MAX     fused batches of at most this many edges (0..16,
+ *                         default 16; 0: never) travel inside the kernel's
+ *                         launch parameters instead of a staging buffer that
+ *                         the kernel reads across the bus. */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -253,7 +263,8 @@ typedef enum {
   RG_OPT_MAX_LEVELS = 9,
   RG_OPT_PULL_GROUPS = 10,
   RG_OPT_FUSED_MAX = 11,
-  RG_OPT_PHASE_TRACE = 12
+  RG_OPT_PHASE_TRACE = 12,
+  RG_OPT_INLINE_MAX = 13
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

@@ -23,7 +23,8 @@
 //   ref_driver rt     <algo> <graph> <V> <root> <rate> <clients,...> <timeout_ms> <max_updates> <out|->
 // algo: bfs | sssp | sswp | wcc.
 // graph: a file in the reference's binary format (core/io.hpp:26-36), or
-//   rmat:<scale>:<seed>            the 16*2^scale-edge RMAT stream of rg_gen_rmat
+//   rmat:<scale>:<seed>            the 16*2^scale-edge RMAT stream of rg_gen_rmat (longer
+//                                  when a window below reaches past its end)
 //   mix:<scale>:<edges>:<seed>     the ER+RMAT mix of rg_gen_er_rmat_mix
 // generated in memory (a/b/c = .57/.19/.19), so no other library is needed;
 // a suffix @<lo>:<hi> keeps edges [lo, hi) of the list only (the window a
@@ -104,7 +105,9 @@ Input load_input(const char *spec_arg) {
   }
   if (sscanf(spec.c_str(), "rmat:%u:%llu", &sc, &seed) == 2) {
     in.scale = sc;
-    in.n = 16ull << sc;
+    // the stream continues past 16 * 2^scale edges when a window reaches beyond
+    // (the generator is counter-based: a longer stream keeps the same prefix)
+    in.n = std::max<unsigned long long>(16ull << sc, window ? hi : 0);
     in.owned.resize(2 * in.n);
     rg_gen_rmat(sc, 0, in.n, 0.57, 0.19, 0.19, seed, in.owned.data());
   } else if (sscanf(spec.c_str(), "mix:%u:%llu:%llu", &sc, &ne, &seed) == 3) {

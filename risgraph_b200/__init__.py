@@ -121,6 +121,7 @@ def _declare(L):
         "rg_level_trace": [P, P, _u64, P, P],
         "rg_level_times": [P, P, _u64, P],
         "rg_phase_trace": [P, P],
+        "rg_level_stamps": [P, P, _u64, P],
         "rg_build_tree_csr_static": [_int, _u64, _u64, _u64, P, P, P, P, P, P],
         "rg_set_option": [P, _int, _u64],
         "rg_get_option": [P, _int, P],
@@ -456,9 +457,18 @@ class Graph:
         _check(lib().rg_level_trace(self._h, _p(sizes), len(sizes), _p(n), _p(e)), "rg_level_trace")
         return sizes, int(e[0])
 
+    def level_device_times(self):
+        """Per level device ms of the last tree call from the level loop's own
+        device-clock stamps (graph-launched calls included)."""
+        n = np.zeros(1, np.uint64)
+        _check(lib().rg_level_stamps(self._h, None, 0, _p(n)), "rg_level_stamps")
+        ns = np.zeros(int(n[0]) + 1, np.uint64)
+        _check(lib().rg_level_stamps(self._h, _p(ns), len(ns), _p(n)), "rg_level_stamps")
+        return np.diff(ns.astype(np.int64)) / 1e6
+
     OPTIONS = {"dense_pull": 0, "dense_div": 1, "lbs_min": 2, "bfs_bottom_up": 3, "recompute_min": 4, "bu_div": 5,
                "pull_div": 6, "tiny_edges": 7, "pull_split": 8, "max_levels": 9,
-               "pull_groups": 10, "fused_max": 11, "phase_trace": 12}
+               "pull_groups": 10, "fused_max": 11, "phase_trace": 12, "inline_max": 13}
 
     # rg_phase_trace's phase words (RG_PH_* in the header), in order
     PHASES = ("begin", "unpack", "lookup", "grow", "write", "count", "old", "seed", "del_repair", "end")

@@ -546,6 +546,21 @@ int rg_level_trace(rg_graph *gh, uint64_t *sizes, uint64_t cap, uint64_t *levels
   return RG_OK;
 }
 
+int rg_level_stamps(rg_graph *gh, uint64_t *ns, uint64_t cap, uint64_t *levels) {
+  int rc = check_graph(gh);
+  if (rc) return rc;
+  Graph &g = gh->g;
+  RG_CUDA(cudaMemcpyAsync(g.h_ctl, g.d.ctl, sizeof(unsigned long long) * rg::C_COUNT, cudaMemcpyDeviceToHost, g.stream));
+  RG_CUDA(cudaStreamSynchronize(g.stream));
+  uint64_t n = std::min<uint64_t>(g.h_ctl[rg::C_LEVEL], rg::TRACE_CAP);
+  if (levels) *levels = n;
+  if (ns && cap) {
+    uint64_t k = std::min(cap, n + 1);
+    RG_CUDA(cudaMemcpy(ns, g.d.trace + rg::TRACE_CAP, k * 8, cudaMemcpyDeviceToHost));
+  }
+  return RG_OK;
+}
+
 int rg_phase_trace(rg_graph *gh, uint64_t *ns) {
   if (!gh || !ns) return RG_EINVAL;
   Graph &g = gh->g;
@@ -598,6 +613,10 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
       g.phase_trace = (int)value;
       g.d.ptrace = value ? g.ptrace_buf : nullptr;
       return RG_OK;
+    case RG_OPT_INLINE_MAX:
+      if (value > rg::INLINE_MAX_EDGES) break;
+      g.inline_max = value;
+      return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -620,6 +639,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_PULL_GROUPS: *value = g.pull_groups; return RG_OK;
     case RG_OPT_FUSED_MAX: *value = g.fused_max; return RG_OK;
     case RG_OPT_PHASE_TRACE: *value = (uint64_t)g.phase_trace; return RG_OK;
+    case RG_OPT_INLINE_MAX: *value = g.inline_max; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

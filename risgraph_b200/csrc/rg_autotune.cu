@@ -138,7 +138,7 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
   }
   if (algo != RG_BFS && (rc = t.tune(RG_OPT_PULL_SPLIT, {0, 1}, &Tuner::build_ms, &ms))) return rc;
   if ((rc = t.tune(RG_OPT_DENSE_DIV, {10, 20, 40, 80}, &Tuner::build_ms, &ms))) return rc;
-  if ((rc = t.tune(RG_OPT_LBS_MIN, {512, 2048, 8192, 32768}, &Tuner::build_ms, &ms))) return rc;
+  if ((rc = t.tune(RG_OPT_LBS_MIN, {512, 2048, 8192, 32768, 131072}, &Tuner::build_ms, &ms))) return rc;
   // small-frontier knob: builds and the sample's round trips together
   if ((rc = t.tune(RG_OPT_TINY_EDGES, {0, 8192, 32768, 131072}, &Tuner::both_ms, &ms))) return rc;
   if ((rc = t.build_ms(&out->build_ms_after))) return rc;
@@ -149,7 +149,7 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
     if ((rc = t.build_ms(&out->build_ms_after))) return rc;
     if ((rc = t.apply_ms(&out->apply_ms_after))) return rc;
   }
-  for (int o = 0; o < NOPT; o++) rg_get_option(g, o, &out->options[o]);
+  for (int o = 0; o <= RG_OPT_INLINE_MAX; o++) rg_get_option(g, o, &out->options[o]);
   out->trials = t.trials;
   // leave the labels of a fresh build, as rg_build_tree would
   return rg_build_tree(g, algo, root, nullptr);

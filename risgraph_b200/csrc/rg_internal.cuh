@@ -242,6 +242,7 @@ struct ApplyHdr {
 constexpr uint64_t APPLY_HDR2 = 64;
 constexpr uint64_t APPLY_DATA_OFF = 128;
 constexpr uint64_t SMALL_EDGES = 2048;  // largest batch of the fused single-CTA apply path
+constexpr uint64_t INLINE_MAX_EDGES = 16;  // largest batch carried in the fused kernel's parameters
 inline uint64_t apply_old_off() { return APPLY_DATA_OFF + 2 * SMALL_EDGES * sizeof(rg_edge); }
 // the delete batch of an insert+delete submission starts here, from APPLY_DATA_OFF
 inline uint64_t apply_data2_off() { return SMALL_EDGES * sizeof(rg_edge); }
@@ -329,6 +330,7 @@ struct Graph {
   // SSSP, larger batches run faster on the grid-wide kernels
   uint64_t fused_max = 2048;
   int phase_trace = 0;            // RG_OPT_PHASE_TRACE
+  uint64_t inline_max = 16;       // RG_OPT_INLINE_MAX: largest fused batch passed in the launch parameters
   unsigned long long *ptrace_buf = nullptr;  // its device buffer (allocated with the labels)
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays

@@ -259,7 +259,8 @@ void run_load(rg_server *s, Instance *in, const rg_load_config &c, Sink &sink, r
         const uint64_t sn = c.offset + issued;
         const bool is_add = (sn & 1) == 0;
         const uint64_t idx = is_add ? c.imported + sn / 2 : sn / 2;
-        if (issued >= limit || (is_add ? idx >= c.n_pairs : idx >= c.imported)) {
+        // (a delete's index is below the insert's before it: the window end bounds both)
+        if (issued >= limit || idx >= c.n_pairs) {
           issuing = false;
           break;
         }

@@ -125,11 +125,16 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long local = 0, scanned = 0;
-  for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
+  // vertices per warp: as few as the frontier allows (at most 32), so that a
+  // frontier smaller than 32 x the grid's warps still spreads over every warp
+  // instead of leaving a few warps to walk 32 lists each
+  const uint64_t per = (n + nwarps - 1) / nwarps;
+  const uint32_t vpw = per >= 32 ? 32u : (per ? (uint32_t)per : 1u);
+  for (uint64_t base = warp * vpw; base < n; base += nwarps * vpw) {
     uint64_t i = base + lane;
     uint32_t u = 0, len = 0;
     uint64_t off = 0, su = 0;
-    if (i < n) {
+    if (lane < vpw && i < n) {
       u = fin[i];
       len = seg_len(g.out, u);
       off = g.out.off[u];
@@ -1051,7 +1056,10 @@ __device__ __forceinline__ void tiny_levels(const DevGraph &g, uint32_t *q_in, u
         if (go) {
           c[C_STAMP] += 1;
           c[C_DEPTH] = lvl;
-          if (lvl < TRACE_CAP) g.trace[lvl] = n;
+          if (lvl < TRACE_CAP) {
+            g.trace[lvl] = n;
+            g.trace[TRACE_CAP + lvl] = global_ns();
+          }
           c[C_LEVEL] = lvl + 1;
           *nxt_n = 0;
         }
@@ -1211,7 +1219,10 @@ __global__ void __launch_bounds__(LVB_TPB) k_level_begin(DevGraph g, const uint3
   c[C_MODE] = mode;
   if (use_switch) c[C_KLAUNCH] += 1 + mode_launches(mode) + (mode == M_PULL ? cfg.pull_groups - 2 : 0);
   if (n) {
-    if (lvl < TRACE_CAP) g.trace[lvl] = n;
+    if (lvl < TRACE_CAP) {
+      g.trace[lvl] = n;
+      g.trace[TRACE_CAP + lvl] = global_ns();  // the level's start on the device clock
+    }
     c[C_LEVEL] = lvl + 1;
   }
   if (use_switch) cudaGraphSetConditional(sw, (unsigned)mode);
@@ -1222,6 +1233,8 @@ __global__ void k_loop_cond(DevGraph g, const unsigned long long *n_after, uint6
   const uint64_t n = *n_after;
   const uint64_t lvl = g.ctl[C_LEVEL];
   g.ctl[C_KLAUNCH] += 1;
+  // the end of the levels so far (the next level's start overwrites it)
+  if (lvl < TRACE_CAP) g.trace[TRACE_CAP + lvl] = global_ns();
   if (n && lvl >= max_levels) atomicCAS(&g.ctl[C_ERR], 0ull, (unsigned long long)RG_ETIMEOUT);
   cudaGraphSetConditional(handle, (n && lvl < max_levels) ? 1u : 0u);
 }
@@ -1886,6 +1899,18 @@ struct StagedBatch {
   unsigned long long stamp;  // C_STAMP at the kernel's start (used by its first batch)
 };
 
+// A batch of at most INLINE_EDGES edges travels inside the kernel's parameters
+// (the launch carries it to the SM), so the kernel reads no staging buffer
+// across the bus: single updates and the served path's small epochs skip the
+// one PCIe round trip (about 6 us) that staging from mapped memory costs.
+// words[] holds the batch as the caller gave it: rg_edge records (3 words per
+// edge) or (src, dst) pairs (2 words).
+constexpr unsigned INLINE_EDGES = INLINE_MAX_EDGES;
+struct InlineBatch {
+  uint64_t n, pairs, want, inv_tag;
+  uint64_t words[3 * INLINE_EDGES];
+};
+
 // The batch crosses the bus in 16-byte loads into device scratch: the first
 // APPLY_SPEC chunks in the same round trip as the header (thread hdr_t reads
 // the header, threads chunk_t .. chunk_t + APPLY_SPEC - 1 the chunks), the
@@ -1911,12 +1936,13 @@ __device__ __forceinline__ void stage_batch(const DevGraph &g, const ApplyHdr *h
 // repair, by all threads of the CTA after a barrier.  Returns 0 when nothing
 // is left, 1 when the repair left work for the graph nodes after the kernel
 // (C_OVER set when the deletion repair handed over), 2 after a storage error
-// or when it skipped the batch.
+// or when it skipped the batch.  inl: the batch's words in the kernel's
+// parameters (an inline batch), or null when they were staged into scratch.
 template <int A, bool W>
 __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, const StagedBatch &sb,
                                            const char *data, uint64_t *old_host, uint32_t *cand, int add, int directed,
                                            uint32_t *q0, uint32_t mst, int second, const FusedRepair &fr,
-                                           uint4 *scratch) {
+                                           uint4 *scratch, const uint64_t *inl = nullptr) {
   __shared__ int s_skip;
   unsigned long long *c = g.ctl;
   const unsigned tid = threadIdx.x;
@@ -1945,22 +1971,23 @@ __device__ __forceinline__ int apply_batch(const DevGraph &g, sdev::OpView ops, 
   const uint64_t nops = directed ? n : 2 * n;
   const int weighted = W ? 1 : 0;
   const uint64_t chunks = (n * (sb.pairs ? 16 : sizeof(rg_edge)) + 15) / 16;
-  if (chunks > APPLY_SPEC) {
+  if (!inl && chunks > APPLY_SPEC) {
     const uint4 *raw = reinterpret_cast<const uint4 *>(data);
     for (uint64_t k = APPLY_SPEC + tid; k < chunks; k += FS_TPB) scratch[k] = __ldcv(&raw[k]);
     __syncthreads();
   }
+  // staged words are read past L1 (this CTA wrote them); inline ones are parameters
+  const uint64_t *words = inl ? inl : reinterpret_cast<const uint64_t *>(scratch);
+  auto word = [&](uint64_t k) -> uint64_t { return inl ? inl[k] : __ldcg(&words[k]); };
   if (sb.pairs) {
-    const uint64_t *p = reinterpret_cast<const uint64_t *>(scratch);
     for (uint64_t i = tid; i < n; i += FS_TPB) {
-      uint64_t s64 = __ldcg(&p[2 * i]), d64 = __ldcg(&p[2 * i + 1]);
+      uint64_t s64 = word(2 * i), d64 = word(2 * i + 1);
       uint32_t w = weighted ? (uint32_t)(splitmix64((s64 << 32) | d64) % 255 + 1) : 0u;
       sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, w, directed);
     }
   } else {
-    const uint64_t *e = reinterpret_cast<const uint64_t *>(scratch);
     for (uint64_t i = tid; i < n; i += FS_TPB) {
-      uint64_t s64 = __ldcg(&e[3 * i]), d64 = __ldcg(&e[3 * i + 1]), w64 = __ldcg(&e[3 * i + 2]);
+      uint64_t s64 = word(3 * i), d64 = word(3 * i + 1), w64 = word(3 * i + 2);
       sdev::put_ops(ops, i, (uint32_t)s64, (uint32_t)d64, weighted ? (uint32_t)w64 : 0u, directed);
     }
   }
@@ -2091,6 +2118,62 @@ __global__ void __launch_bounds__(FS_TPB)
   unsigned long long lf = r == 1 ? 1 : 0;
   if (r == 0) {
     r = apply_batch<A, W>(g, ops, sb2, data2, nullptr, cand, 0, directed, q0, mst, 1, fr, scratch2);
+    lf = r == 1 ? 2 : 0;
+  }
+  if (threadIdx.x == 0) g.ctl[C_LEFT] = lf;
+  ctl_to_host(g, ctl_host);
+}
+
+// The header of an inline batch (its size clamped to what the parameters hold).
+__device__ __forceinline__ void inline_header(const DevGraph &g, const InlineBatch &ib, StagedBatch &sb) {
+  if (threadIdx.x == 0) {
+    sb.stamp = g.ctl[C_STAMP];
+    sb.n = ib.n < INLINE_EDGES ? ib.n : INLINE_EDGES;
+    sb.pairs = ib.pairs;
+    sb.want = ib.want;
+    sb.inv_tag = ib.inv_tag;
+  }
+}
+
+// k_apply_small for an inline batch (launched directly, not from a graph).
+template <int A, bool W>
+__global__ void __launch_bounds__(FS_TPB)
+    k_apply_small_inl(DevGraph g, sdev::OpView ops, const __grid_constant__ InlineBatch ib, uint64_t *old_host,
+                      uint32_t *cand, int add, int directed, uint32_t *q0, uint32_t mst, FusedRepair fr,
+                      unsigned long long *ctl_host) {
+  __shared__ StagedBatch sb;
+  if (g.ptrace && threadIdx.x == 0) {
+    g.ptrace[32] = g.ptrace[33] = global_ns();
+    g.ptrace[15] = 0;
+    g.ptrace[31] = 0;
+  }
+  inline_header(g, ib, sb);
+  __syncthreads();
+  const int r = apply_batch<A, W>(g, ops, sb, nullptr, old_host, cand, add, directed, q0, mst, 0, fr, nullptr, ib.words);
+  if (threadIdx.x == 0) g.ctl[C_LEFT] = r == 1 ? (add ? 1 : 2) : 0;
+  ctl_to_host(g, ctl_host);
+}
+
+// k_apply_mixed for two inline batches.  When the insert batch leaves work,
+// the host continues exactly as after k_apply_mixed: the delete batch is in
+// the staging buffer too (the host wrote it there before the launch).
+template <int A, bool W>
+__global__ void __launch_bounds__(FS_TPB)
+    k_apply_mixed_inl(DevGraph g, sdev::OpView ops, const __grid_constant__ InlineBatch ib1,
+                      const __grid_constant__ InlineBatch ib2, uint32_t *cand, int directed, uint32_t *q0,
+                      uint32_t mst, FusedRepair fr, unsigned long long *ctl_host) {
+  __shared__ StagedBatch sb1, sb2;
+  if (g.ptrace && threadIdx.x == 0) {
+    g.ptrace[32] = g.ptrace[33] = g.ptrace[34] = g.ptrace[35] = global_ns();
+    g.ptrace[15] = g.ptrace[31] = 0;
+  }
+  inline_header(g, ib1, sb1);
+  inline_header(g, ib2, sb2);
+  __syncthreads();
+  int r = apply_batch<A, W>(g, ops, sb1, nullptr, nullptr, cand, 1, directed, q0, mst, 0, fr, nullptr, ib1.words);
+  unsigned long long lf = r == 1 ? 1 : 0;
+  if (r == 0) {
+    r = apply_batch<A, W>(g, ops, sb2, nullptr, nullptr, cand, 0, directed, q0, mst, 1, fr, nullptr, ib2.words);
     lf = r == 1 ? 2 : 0;
   }
   if (threadIdx.x == 0) g.ctl[C_LEFT] = lf;
@@ -2908,7 +2991,8 @@ int tree_alloc(Graph &g) {
     unsigned long long one = 1;
     RG_CUDA(cudaMemcpy(&g.d.ctl[C_MODEPOCH], &one, 8, cudaMemcpyHostToDevice));
   }
-  if ((rc = alloc((void **)&g.d.trace, TRACE_CAP * 8, "level trace"))) return rc;
+  // frontier sizes, then the levels' start stamps (one more: the end of the last)
+  if ((rc = alloc((void **)&g.d.trace, (2 * TRACE_CAP + 1) * 8, "level trace"))) return rc;
   if ((rc = alloc((void **)&g.ptrace_buf, RG_PHASE_SLOTS * 8, "phase trace"))) return rc;
   RG_CUDA(cudaMemset(g.ptrace_buf, 0, RG_PHASE_SLOTS * 8));
   g.d.ptrace = g.phase_trace ? g.ptrace_buf : nullptr;
@@ -3120,6 +3204,42 @@ int finish_left(Graph &g, unsigned long long left) {
   return read_ctl(g);
 }
 
+// An inline batch from the caller's edges (n <= INLINE_EDGES).
+InlineBatch inline_batch(const void *src, uint64_t n, bool pairs, bool want, uint64_t inv_tag) {
+  InlineBatch ib;
+  ib.n = n;
+  ib.pairs = pairs ? 1 : 0;
+  ib.want = want ? 1 : 0;
+  ib.inv_tag = inv_tag;
+  std::memset(ib.words, 0, sizeof(ib.words));
+  std::memcpy(ib.words, src, n * (pairs ? 16 : sizeof(rg_edge)));
+  return ib;
+}
+
+// One batch of at most INLINE_EDGES edges: k_apply_small_inl, launched
+// directly with the batch in its parameters.
+template <int A, bool W>
+int launch_apply_inline(Graph &g, const InlineBatch &ib, bool add, int directed) {
+  const LevelCfg cfg = level_cfg(g, A, false);
+  uint64_t *old_host = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(g.stage_host_dev) + apply_old_off());
+  k_apply_small_inl<A, W><<<1, FS_TPB, 0, g.stream>>>(g.d, sdev::op_view(g), ib, old_host, op_cand(g), add ? 1 : 0,
+                                                      directed ? 1 : 0, g.q[0], mod_stamp(g), fused_repair(g, cfg),
+                                                      g.h_ctl_dev);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
+}
+
+// An insert batch and a delete batch of at most INLINE_EDGES edges each:
+// k_apply_mixed_inl.
+template <int A, bool W>
+int launch_mixed_inline(Graph &g, const InlineBatch &ib1, const InlineBatch &ib2, int directed) {
+  const LevelCfg cfg = level_cfg(g, A, false);
+  k_apply_mixed_inl<A, W><<<1, FS_TPB, 0, g.stream>>>(g.d, sdev::op_view(g), ib1, ib2, op_cand(g), directed ? 1 : 0,
+                                                      g.q[0], mod_stamp(g), fused_repair(g, cfg), g.h_ctl_dev);
+  RG_CUDA(cudaGetLastError());
+  return RG_OK;
+}
+
 template <int A, bool W>
 int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_t n, int directed, bool add,
                   uint64_t *old_num) {
@@ -3145,10 +3265,16 @@ int apply_small_t(Graph &g, const rg_edge *edges, const uint64_t *pairs, uint64_
     h->inv_tag = 2ull * g.inv_epoch;  // tag: invalidated; tag+1: rescued
   }
   reset_stats(g);
-  cudaGraphExec_t exec;
-  if ((rc = apply_exec<A, W>(g, add, directed, &exec))) return rc;
   count_launch(g);
-  RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  if (n <= g.inline_max) {
+    const InlineBatch ib = inline_batch(pairs ? (const void *)pairs : (const void *)edges, n, pairs != nullptr,
+                                        old_num != nullptr, h->inv_tag);
+    if ((rc = launch_apply_inline<A, W>(g, ib, add, directed))) return rc;
+  } else {
+    cudaGraphExec_t exec;
+    if ((rc = apply_exec<A, W>(g, add, directed, &exec))) return rc;
+    RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  }
   RG_CUDA(cudaStreamSynchronize(g.stream));
   const int what = add ? 1 : 2;
   bool replayed = false;
@@ -3191,10 +3317,18 @@ int apply_add_del_t(Graph &g, const rg_edge *adds, uint64_t n_add, const rg_edge
   }
   h2->inv_tag = 2ull * g.inv_epoch;
   reset_stats(g);
-  cudaGraphExec_t exec;
-  if ((rc = mixed_exec<A, W>(g, directed, &exec))) return rc;
   count_launch(g);
-  RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  if (n_add <= g.inline_max && n_del <= g.inline_max) {
+    // both batches in the parameters; the staging buffer keeps them too for
+    // the graphs that run when the insert batch leaves work
+    const InlineBatch ib1 = inline_batch(adds, n_add, false, false, 0);
+    const InlineBatch ib2 = inline_batch(dels, n_del, false, false, h2->inv_tag);
+    if ((rc = launch_mixed_inline<A, W>(g, ib1, ib2, directed))) return rc;
+  } else {
+    cudaGraphExec_t exec;
+    if ((rc = mixed_exec<A, W>(g, directed, &exec))) return rc;
+    RG_CUDA(cudaGraphLaunch(exec, g.stream));
+  }
   RG_CUDA(cudaStreamSynchronize(g.stream));
   if (g.h_ctl[C_ERR] == RG_ENOSPACE && g.h_ctl[C_AUX] == 1) {
     // the insert phase ran out of pool during growth (the delete phase did not
