@@ -249,7 +249,14 @@ int rg_phase_trace(rg_graph *g, uint64_t *ns);
  *   RG_OPT_INLINE_MAX     fused batches of at most this many edges (0..16,
  *                         default 16; 0: never) travel inside the kernel's
  *                         launch parameters instead of a staging buffer that
- *                         the kernel reads across the bus. */
+ *                         the kernel reads across the bus.
+ *   RG_OPT_CLUSTER_EDGES  frontiers too large for one CTA but of at most 16 x
+ *                         1024 vertices (8 x 1024 where the GPU schedules no
+ *                         16-CTA cluster) and this many out-slots (default
+ *                         65536, at most 2^20; 0: never) run their levels in
+ *                         one thread-block cluster, one launch for successive
+ *                         levels; a frontier that a tiny level could take goes
+ *                         to the cluster when it has more than 4096 slots. */
 typedef enum {
   RG_OPT_DENSE_PULL = 0,
   RG_OPT_DENSE_DIV = 1,
@@ -264,7 +271,8 @@ typedef enum {
   RG_OPT_PULL_GROUPS = 10,
   RG_OPT_FUSED_MAX = 11,
   RG_OPT_PHASE_TRACE = 12,
-  RG_OPT_INLINE_MAX = 13
+  RG_OPT_INLINE_MAX = 13,
+  RG_OPT_CLUSTER_EDGES = 14
 } rg_option;
 int rg_set_option(rg_graph *g, int option, uint64_t value);
 int rg_get_option(rg_graph *g, int option, uint64_t *value);

@@ -468,7 +468,7 @@ class Graph:
 
     OPTIONS = {"dense_pull": 0, "dense_div": 1, "lbs_min": 2, "bfs_bottom_up": 3, "recompute_min": 4, "bu_div": 5,
                "pull_div": 6, "tiny_edges": 7, "pull_split": 8, "max_levels": 9,
-               "pull_groups": 10, "fused_max": 11, "phase_trace": 12, "inline_max": 13}
+               "pull_groups": 10, "fused_max": 11, "phase_trace": 12, "inline_max": 13, "cluster_edges": 14}
 
     # rg_phase_trace's phase words (RG_PH_* in the header), in order
     PHASES = ("begin", "unpack", "lookup", "grow", "write", "count", "old", "seed", "del_repair", "end")

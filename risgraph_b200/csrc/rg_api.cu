@@ -617,6 +617,10 @@ int rg_set_option(rg_graph *gh, int option, uint64_t value) {
       if (value > rg::INLINE_MAX_EDGES) break;
       g.inline_max = value;
       return RG_OK;
+    case RG_OPT_CLUSTER_EDGES:
+      if (value > (1ull << 20)) break;
+      g.cluster_edges = value;
+      return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;
@@ -640,6 +644,7 @@ int rg_get_option(rg_graph *gh, int option, uint64_t *value) {
     case RG_OPT_FUSED_MAX: *value = g.fused_max; return RG_OK;
     case RG_OPT_PHASE_TRACE: *value = (uint64_t)g.phase_trace; return RG_OK;
     case RG_OPT_INLINE_MAX: *value = g.inline_max; return RG_OK;
+    case RG_OPT_CLUSTER_EDGES: *value = g.cluster_edges; return RG_OK;
   }
   rg::set_error("unknown option");
   return RG_EINVAL;

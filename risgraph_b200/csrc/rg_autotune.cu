@@ -126,7 +126,7 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
   *out = rg_tune_report{};
   if ((rc = t.build_ms(&out->build_ms_before))) return rc;
   if ((rc = t.apply_ms(&out->apply_ms_before))) return rc;
-  constexpr int NOPT = RG_OPT_PULL_GROUPS + 1;
+  constexpr int NOPT = RG_OPT_CLUSTER_EDGES + 1;
   uint64_t orig[NOPT];
   for (int o = 0; o < NOPT; o++) rg_get_option(g, o, &orig[o]);
   double ms = 0;
@@ -141,6 +141,8 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
   if ((rc = t.tune(RG_OPT_LBS_MIN, {512, 2048, 8192, 32768, 131072}, &Tuner::build_ms, &ms))) return rc;
   // small-frontier knob: builds and the sample's round trips together
   if ((rc = t.tune(RG_OPT_TINY_EDGES, {0, 8192, 32768, 131072}, &Tuner::both_ms, &ms))) return rc;
+  // mid-size frontiers in one thread-block cluster: builds and round trips together
+  if ((rc = t.tune(RG_OPT_CLUSTER_EDGES, {0, 16384, 65536, 262144}, &Tuner::both_ms, &ms))) return rc;
   if ((rc = t.build_ms(&out->build_ms_after))) return rc;
   if ((rc = t.apply_ms(&out->apply_ms_after))) return rc;
   if (out->build_ms_after + out->apply_ms_after > 1.05 * (out->build_ms_before + out->apply_ms_before)) {
@@ -149,7 +151,7 @@ extern "C" int rg_autotune(rg_graph *g, int algo, uint64_t root, const rg_edge *
     if ((rc = t.build_ms(&out->build_ms_after))) return rc;
     if ((rc = t.apply_ms(&out->apply_ms_after))) return rc;
   }
-  for (int o = 0; o <= RG_OPT_INLINE_MAX; o++) rg_get_option(g, o, &out->options[o]);
+  for (int o = 0; o <= RG_OPT_CLUSTER_EDGES; o++) rg_get_option(g, o, &out->options[o]);
   out->trials = t.trials;
   // leave the labels of a fresh build, as rg_build_tree would
   return rg_build_tree(g, algo, root, nullptr);

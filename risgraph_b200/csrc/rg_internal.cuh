@@ -83,7 +83,8 @@ enum LevelMode : unsigned long long {
   M_BOTTOM_UP = 4,  // k_bfs_bottom_up (full BFS builds)
   M_LBS = 5,        // edge-balanced push (degree scan + tile partition + k_push_lbs)
   M_TINY = 6,       // k_push_tiny: one CTA runs successive small levels
-  M_COUNT = 7
+  M_CLUSTER = 7,    // k_push_cluster: one thread-block cluster runs successive mid-size levels
+  M_COUNT = 8
 };
 constexpr int TRACE_CAP = 4096;
 
@@ -331,6 +332,8 @@ struct Graph {
   uint64_t fused_max = 2048;
   int phase_trace = 0;            // RG_OPT_PHASE_TRACE
   uint64_t inline_max = 16;       // RG_OPT_INLINE_MAX: largest fused batch passed in the launch parameters
+  uint64_t cluster_edges = 65536;  // RG_OPT_CLUSTER_EDGES: out-slot limit of a cluster level (0: off)
+  int cl_ctas = 0;                  // CTAs of the cluster kernel (16 where the GPU schedules it, else 8)
   unsigned long long *ptrace_buf = nullptr;  // its device buffer (allocated with the labels)
   int bfs_bottom_up = 1;
   uint64_t bu_div = 64;  // measured on RMAT-22: the second BFS level (2% of |V|, most edges) already pays

@@ -22,6 +22,7 @@
 #include <cstring>
 #include <type_traits>
 
+#include <cooperative_groups.h>
 #include <cub/block/block_reduce.cuh>
 #include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
@@ -1118,6 +1119,148 @@ __global__ void __launch_bounds__(TINY_TPB) k_push_tiny(DevGraph g, uint32_t *q_
   tiny_levels<A, W>(g, q_in, n_in, q_out, n_out, q_out, n_out, max_levels, max_edges, mst, true);
 }
 
+// ---- cluster levels ------------------------------------------------------------
+// A frontier too large for one CTA but at most CL_TPB vertices per CTA of a
+// thread-block cluster (16 CTAs where the GPU schedules a cluster that size,
+// else 8; one per SM) runs in k_push_cluster: successive levels inside one
+// launch, separated by the hardware cluster barrier (barrier.cluster, with
+// release/acquire ordering of the global queue and labels) instead of kernel
+// boundaries and a conditional node per level, which cost 25-40 us per
+// mid-size level in the graph-driven loop.  Each CTA stages CL_TPB frontier
+// vertices (offset, value, degree prefix) in its shared memory; the level's
+// out-slots are spread evenly over every thread of the cluster, and a thread
+// finds the vertex of its slot in the owning CTA's shared memory through
+// distributed shared memory.  Every decision that ends the loop is made from
+// values that all CTAs read alike (the frontier size after a barrier, the
+// CTAs' slot totals in global memory), so that every CTA passes the same
+// barriers.  The loop ends when the frontier empties or outgrows the cluster
+// (more than CL_TPB vertices per CTA or max_edges slots), leaving the frontier
+// in the level's output queue like tiny_levels.
+constexpr int CL_TPB = 1024;
+constexpr int CL_MAX_CTAS = 16;
+constexpr uint64_t CL_EDGES = 1ull << 20;  // largest slot limit of a cluster level
+
+template <int A, bool W>
+__global__ void __launch_bounds__(CL_TPB, 1)
+    k_push_cluster(DevGraph g, uint32_t *q_in, unsigned long long *n_in, uint32_t *q_out, unsigned long long *n_out,
+                   unsigned long long *tot, uint64_t max_levels, uint64_t max_edges, uint32_t mst) {
+  namespace cgr = cooperative_groups;
+  if (g.ctl[C_MODE] != M_CLUSTER) return;  // the same in every CTA
+  cgr::cluster_group cluster = cgr::this_cluster();
+  using P_ = PoolT<W>;
+  using Scan = cub::BlockScan<uint32_t, CL_TPB>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ uint32_t s_pref[CL_TPB + 1];
+  __shared__ uint32_t s_v[CL_TPB];
+  __shared__ uint64_t s_off[CL_TPB];
+  __shared__ uint32_t s_su[CL_TPB];
+  __shared__ uint64_t s_base[CL_MAX_CTAS + 1];
+  const typename P_::E *pool = reinterpret_cast<const typename P_::E *>(g.out.pool);
+  unsigned long long *c = g.ctl;
+  const unsigned tid = threadIdx.x;
+  const unsigned nc = cluster.num_blocks(), r = cluster.block_rank();
+  const uint64_t cap = (uint64_t)nc * CL_TPB;  // frontier vertices the cluster stages
+  uint32_t *cur = q_in, *nxt = q_out;
+  unsigned long long *cur_n = n_in, *nxt_n = n_out;
+  unsigned long long local = 0, scanned = 0;
+  uint64_t n = 0;
+  for (bool first = true;; first = false) {
+    // values every CTA reads alike: written before the last barrier (or the launch)
+    n = __ldcg(cur_n);
+    const unsigned long long st0 = __ldcg(&c[C_STAMP]), lvl = __ldcg(&c[C_LEVEL]);
+    const bool book = !first;  // k_level_begin did the first level's bookkeeping
+    const uint64_t i = (uint64_t)r * CL_TPB + tid;
+    uint32_t d = 0;
+    if (n <= cap && i < n) {
+      const uint32_t u = __ldcg(&cur[i]);
+      s_v[tid] = u;
+      s_off[tid] = g.out.off[u];
+      s_su[tid] = (uint32_t)ld_v32(g.val32, u);
+      d = seg_len(g.out, u);
+    }
+    uint32_t excl, total;
+    Scan(scan_tmp).ExclusiveSum(d, excl, total);
+    s_pref[tid] = excl;
+    if (tid == 0) {
+      s_pref[CL_TPB] = total;
+      tot[r] = total;
+      // the output count: the input of the level before this one, read by every CTA
+      // before the last barrier
+      if (r == 0 && book) *nxt_n = 0;
+    }
+    cluster.sync();  // A: totals and stage visible, output count cleared
+    if (tid < 32) {
+      // the CTAs' slot totals, loaded together and scanned in one warp
+      const uint64_t t = tid < nc ? __ldcg(&tot[tid]) : 0;
+      uint64_t incl = t;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(FULL, incl, o);
+        if (tid >= (unsigned)o) incl += y;
+      }
+      if (tid <= nc) s_base[tid] = incl - t;  // entry nc: the level's slots
+    }
+    __syncthreads();
+    const uint64_t S = s_base[nc];
+    const bool go = n > 0 && n <= cap && (first || (S <= max_edges && lvl < max_levels));
+    if (!go) break;  // the same in every CTA
+    if (book && r == 0 && tid == 0) {
+      c[C_STAMP] = st0 + 1;
+      c[C_DEPTH] = lvl;
+      if (lvl < TRACE_CAP) {
+        g.trace[lvl] = n;
+        g.trace[TRACE_CAP + lvl] = global_ns();
+      }
+      c[C_LEVEL] = lvl + 1;
+    }
+    const uint32_t st = (uint32_t)(book ? st0 + 1 : st0);
+    for (uint64_t base = 0; base < S; base += cap) {
+      const uint64_t e = base + i;
+      bool upd = false;
+      uint32_t v = 0;
+      if (e < S) {
+        unsigned k = 0;  // the CTA that staged slot e: largest k with s_base[k] <= e
+        while (k + 1 < nc && s_base[k + 1] <= e) k++;
+        const uint32_t el = (uint32_t)(e - s_base[k]);
+        const uint32_t *rp = cluster.map_shared_rank(s_pref, k);
+        const uint64_t left = n - (uint64_t)k * CL_TPB;
+        const uint64_t nk = left < CL_TPB ? left : CL_TPB;
+        uint32_t lo = 0, hi = (uint32_t)nk - 1;  // largest j with rp[j] <= el
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) >> 1;
+          if (rp[mid] <= el) lo = mid;
+          else hi = mid - 1;
+        }
+        const uint64_t off = *cluster.map_shared_rank(&s_off[lo], k);
+        const uint32_t u = *cluster.map_shared_rank(&s_v[lo], k);
+        const uint32_t su = *cluster.map_shared_rank(&s_su[lo], k);
+        const typename P_::E ent = __ldg(&pool[off + (el - rp[lo])]);
+        v = P_::nbr(ent);
+        scanned++;
+        if (!(v & DEAD)) upd = relax_lab<A>(g, u, su, v, P_::wt(ent));
+      }
+      local += upd;
+      const bool app = upd && atomicExch(&g.stamp[v], st) != st;
+      warp_append(app, v, nxt, nxt_n, FULL);
+      if (mst) mark_modified(g, upd, v, mst);
+    }
+    cluster.sync();  // B: this level's queue and labels visible; nobody reads a peer's stage any more
+    uint32_t *t = cur;
+    cur = nxt;
+    nxt = t;
+    unsigned long long *tn = cur_n;
+    cur_n = nxt_n;
+    nxt_n = tn;
+  }
+  // the frontier that ended the loop goes to the launch's output queue
+  if (cur != q_out) {
+    for (uint64_t k = (uint64_t)r * CL_TPB + tid; k < n; k += cap) q_out[k] = __ldcg(&cur[k]);
+    if (r == 0 && tid == 0) *n_out = n;
+  }
+  warp_add_result(local, &c[C_RESULT]);
+  warp_add_result(scanned, &c[C_EDGES]);
+}
+
 // ---- device-driven level loop ------------------------------------------------
 // A tree call runs k_prologue, its seed kernel, then a CUDA graph whose WHILE
 // node repeats a pair of levels (queue 0 -> 1, then 1 -> 0).  Each level
@@ -1160,6 +1303,7 @@ __host__ __device__ __forceinline__ int mode_launches(unsigned long long mode) {
     case M_BOTTOM_UP: return 1;
     case M_LBS: return 5;
     case M_TINY: return 1;
+    case M_CLUSTER: return 1;
   }
   return 0;
 }
@@ -1173,6 +1317,8 @@ struct LevelCfg {
   uint64_t tiny_edges;
   uint64_t max_levels;  // level bound baked into the loop graphs
   uint64_t pull_groups;  // launches of a split pull level
+  uint64_t cl_edges;     // out-slot limit of a cluster level (0: no cluster levels)
+  uint64_t cl_v;         // frontier vertices a cluster stages (its CTAs x CL_TPB)
   int allow_pull;
   int bottom_up;
 };
@@ -1180,23 +1326,37 @@ struct LevelCfg {
 // Picks the level mode from the frontier size (the reference's push/pull rule
 // at core/graph.hpp:334 and its vertex/edge-centric rule at :595-612 play the
 // same role); inside a graph it also selects the SWITCH case to run.
-constexpr int LVB_TPB = 256;  // threads of k_level_begin (they sum small frontiers' degrees)
+constexpr int LVB_TPB = 1024;  // threads of k_level_begin (they sum small frontiers' degrees)
+// A frontier that both a tiny level and a cluster level could take goes to the
+// cluster when it has more out-slots than this: one CTA walks them
+// 1024 at a time, the cluster 16,384 at a time.
+constexpr uint64_t CL_TINY_PREF = 4096;
 
 __global__ void __launch_bounds__(LVB_TPB) k_level_begin(DevGraph g, const uint32_t *fin,
                                                          const unsigned long long *fin_n, unsigned long long *fout_n,
                                                          LevelCfg cfg, int use_switch, cudaGraphConditionalHandle sw) {
-  __shared__ unsigned long long s_edges;
+  using BR = cub::BlockReduce<unsigned long long, LVB_TPB>;
+  __shared__ typename BR::TempStorage br_tmp;
   const uint64_t n0 = *fin_n;
-  if (threadIdx.x == 0) s_edges = 0;
-  __syncthreads();
-  if (cfg.tiny_edges && n0 && n0 <= TINY_N) {
-    unsigned long long d = 0;
-    for (uint64_t i = threadIdx.x; i < n0; i += LVB_TPB) d += seg_len(g.out, fin[i]);
-    if (d) atomicAdd(&s_edges, d);
+  unsigned long long d = 0;
+  if ((cfg.tiny_edges && n0 && n0 <= TINY_N) || (cfg.cl_edges && n0 && n0 <= cfg.cl_v)) {
+    // four frontier entries per thread in flight (a frontier of up to 16K vertices)
+    for (uint64_t i0 = threadIdx.x; i0 < n0; i0 += 4 * LVB_TPB) {
+      uint32_t u[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint64_t i = i0 + (uint64_t)k * LVB_TPB;
+        u[k] = i < n0 ? fin[i] : NONE;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) d += u[k] != NONE ? seg_len(g.out, u[k]) : 0u;
+    }
   }
-  __syncthreads();
+  // a tree reduction: 1024 threads adding into one shared word contend for it
+  const unsigned long long s_edges = BR(br_tmp).Sum(d);  // valid in thread 0
   if (threadIdx.x != 0) return;
   const bool tiny = cfg.tiny_edges && n0 && n0 <= TINY_N && s_edges <= cfg.tiny_edges;
+  const bool clus = cfg.cl_edges && n0 && n0 <= cfg.cl_v && s_edges <= cfg.cl_edges;
   unsigned long long *c = g.ctl;
   const uint64_t n = n0;
   const uint64_t lvl = c[C_LEVEL];
@@ -1212,7 +1372,8 @@ __global__ void __launch_bounds__(LVB_TPB) k_level_begin(DevGraph g, const uint3
   // falls below 4x that (the frontier's first large levels are hub-heavy, its
   // last ones are not: the direction switch of Beamer et al., by vertex count)
   else if (cfg.allow_pull && n * (c[C_MODE] == M_PULL ? (cfg.pull_div + 3) / 4 : cfg.pull_div) >= g.V) mode = M_PULL;
-  else if (tiny) mode = M_TINY;
+  else if (tiny && !(clus && s_edges > CL_TINY_PREF)) mode = M_TINY;
+  else if (clus) mode = M_CLUSTER;
   else if (dense) mode = M_DENSE_PUSH;
   else if (n >= cfg.lbs_min) mode = M_LBS;
   if (mode == M_DENSE_PUSH) c[C_ACT] += 1;
@@ -2465,6 +2626,26 @@ int enqueue_mode(Graph &g, cudaStream_t s, int half, unsigned long long mode) {
     case M_BOTTOM_UP:
       k_bfs_bottom_up<W><<<g.num_sms * 8, TPB, 0, s>>>(g.d, fout, fout_n);
       break;
+    case M_CLUSTER: {
+      if (!g.cl_ctas) break;  // never selected then
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3((unsigned)g.cl_ctas);
+      lc.blockDim = dim3(CL_TPB);
+      lc.stream = s;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = (unsigned)g.cl_ctas;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      uint32_t *qi = g.q[half], *qo = g.q[half ^ 1];
+      if (cudaLaunchKernelEx(&lc, k_push_cluster<A, W>, g.d, qi, fin_n, qo, fout_n,
+                             reinterpret_cast<unsigned long long *>(g.lb_sums), max_levels_of(g),
+                             std::min<uint64_t>(g.cluster_edges, CL_EDGES), mst) != cudaSuccess)
+        return RG_ECUDA;
+      break;
+    }
     case M_LBS:
       k_scan_sums<<<SC_BLOCKS, SC_TPB, 0, s>>>(g.d, fin, fin_n, g.scratch64, g.lb_sums);
       k_scan_top<<<1, SC_BLOCKS, 0, s>>>(g.lb_sums);
@@ -2488,6 +2669,8 @@ uint64_t cfg_key(const LevelCfg &c) {
   h = splitmix64(h ^ c.tiny_edges);
   h = splitmix64(h ^ c.max_levels);
   h = splitmix64(h ^ c.pull_groups);
+  h = splitmix64(h ^ c.cl_edges);
+  h = splitmix64(h ^ c.cl_v);
   return splitmix64(h ^ ((uint64_t)c.allow_pull << 1) ^ (uint64_t)c.bottom_up);
 }
 
@@ -2503,6 +2686,8 @@ LevelCfg level_cfg(const Graph &g, int A, bool build_variant) {
   cfg.tiny_edges = g.tiny_edges < TINY_EDGES ? g.tiny_edges : TINY_EDGES;
   cfg.max_levels = max_levels_of(g);
   cfg.pull_groups = cfg.pull_split ? std::max<uint64_t>(2, g.pull_groups) : 2;
+  cfg.cl_edges = g.cl_ctas ? std::min<uint64_t>(g.cluster_edges, CL_EDGES) : 0;
+  cfg.cl_v = (uint64_t)g.cl_ctas * CL_TPB;
   return cfg;
 }
 
@@ -2561,6 +2746,7 @@ int add_level_loop(Graph &g, cudaGraph_t graph, const cudaGraphNode_t *deps, siz
       for (unsigned long long m = 1; m < M_COUNT && e == cudaSuccess && !rc; m++) {
         if (m == M_PULL && !cfg.allow_pull) continue;
         if (m == M_BOTTOM_UP && !cfg.bottom_up) continue;
+        if (m == M_CLUSTER && !cfg.cl_edges) continue;
         cudaGraph_t cg = sp.conditional.phGraph_out[m];
         if ((e = cudaStreamBeginCaptureToGraph(g.cap_stream, cg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
             cudaSuccess)
@@ -2946,8 +3132,50 @@ int dispatch(Graph &g, int algo, int what, uint64_t a, int directed, bool from_c
 
 }  // namespace
 
+// CTAs of the cluster-level kernel: 16 where this GPU schedules a cluster of
+// sixteen 1024-thread CTAs, else the portable 8; 0 (cluster levels off) when
+// neither can run.
+template <int A, bool W>
+void cluster_allow(cudaError_t &e) {
+  cudaError_t x = cudaFuncSetAttribute(k_push_cluster<A, W>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (x != cudaSuccess) e = x;
+}
+
+static void cluster_setup(Graph &g) {
+  cudaError_t e = cudaSuccess;
+  cluster_allow<RG_BFS, false>(e);
+  cluster_allow<RG_BFS, true>(e);
+  cluster_allow<RG_SSSP, false>(e);
+  cluster_allow<RG_SSSP, true>(e);
+  cluster_allow<RG_SSWP, false>(e);
+  cluster_allow<RG_SSWP, true>(e);
+  cluster_allow<RG_WCC, false>(e);
+  cluster_allow<RG_WCC, true>(e);
+  g.cl_ctas = 0;
+  for (int n : {CL_MAX_CTAS, 8}) {
+    if (e != cudaSuccess && n > 8) continue;  // without the attribute only the portable size
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)n);
+    lc.blockDim = dim3(CL_TPB);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)n;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_push_cluster<RG_SSSP, true>, &lc) == cudaSuccess && clusters > 0) {
+      g.cl_ctas = n;
+      break;
+    }
+  }
+  cudaGetLastError();
+}
+
 int tree_alloc(Graph &g) {
   uint64_t V = g.V;
+  cluster_setup(g);
   auto alloc = [&](void **p, size_t bytes, const char *what) -> int {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {

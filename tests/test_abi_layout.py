@@ -80,7 +80,7 @@ def test_option_names_match_header_enum():
              "bfs_bottom_up": "BFS_BOTTOM_UP", "recompute_min": "RECOMPUTE_MIN", "bu_div": "BFS_BU_DIV",
              "pull_div": "PULL_DIV", "tiny_edges": "TINY_EDGES", "pull_split": "PULL_SPLIT",
              "max_levels": "MAX_LEVELS", "pull_groups": "PULL_GROUPS",
-             "fused_max": "FUSED_MAX", "phase_trace": "PHASE_TRACE", "inline_max": "INLINE_MAX"}
+             "fused_max": "FUSED_MAX", "phase_trace": "PHASE_TRACE", "inline_max": "INLINE_MAX", "cluster_edges": "CLUSTER_EDGES"}
     assert set(py) == set(names), set(py) ^ set(names)
     for k, v in py.items():
         assert header[names[k]] == v, k

@@ -88,6 +88,8 @@ PUSH_MODES = {
     "edge_balanced": {"lbs_min": 1, "dense_div": 1},
     "dense": {"dense_div": 1 << 30},
     "sparse": {"lbs_min": 1 << 40, "dense_div": 1},
+    # successive levels in one thread-block cluster (the graph's frontiers all fit)
+    "cluster": {"cluster_edges": 1 << 20},
 }
 
 
@@ -95,15 +97,15 @@ PUSH_MODES = {
 @pytest.mark.parametrize("mode", sorted(PUSH_MODES))
 def test_build_tree_parity_push_modes(algo, mode):
     """Builds pushed level by level in one mode: the edge-balanced and dense
-    modes commit each level through per-vertex packed keys, the sparse mode
-    through the 16-byte CAS; values equal the oracle's, trees are valid, and
-    an incremental batch on top still matches."""
+    modes commit each level through per-vertex packed keys, the sparse and
+    cluster modes through the 16-byte CAS; values equal the oracle's, trees
+    are valid, and an incremental batch on top still matches."""
     scale = 13
     V = 1 << scale
     pairs = gen.er_rmat_mix(scale, 24 * V, seed=17)
     root = gen.max_out_degree_vertex(pairs, V)
     g = gpu_graph(algo, V, pairs)
-    for k, v in {"dense_pull": 0, "bfs_bottom_up": 0, "tiny_edges": 0, **PUSH_MODES[mode]}.items():
+    for k, v in {"dense_pull": 0, "bfs_bottom_up": 0, "tiny_edges": 0, "cluster_edges": 0, **PUSH_MODES[mode]}.items():
         g.set_option(k, v)
     og = oracle_graph(algo, V, pairs)
     og.build_tree(root)
@@ -570,3 +572,38 @@ def test_autotune_keeps_values(algo):
     og.build_tree(root)
     np.testing.assert_array_equal(g.values(), og.labels()[0])
     check_tree(g, og, root)
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("cluster_edges", [0, 16384, 1 << 20])
+def test_cluster_levels_in_builds_and_batches(algo, cluster_edges):
+    """Mid-size frontiers run in one thread-block cluster (RG_OPT_CLUSTER_EDGES):
+    off, with a slot limit that some levels pass (the loop leaves the cluster
+    mid-way and the level loop carries on), and for every level that fits.
+    A build, then sliding-window batches whose repairs use the same loop,
+    match the oracle after every batch; the level trace stays in order."""
+    scale = 14
+    pairs = gen.rmat(scale, seed=71)
+    V = 1 << scale
+    imported = int(len(pairs) * 0.9)
+    directed = algo != "wcc"
+    root = 0 if algo == "wcc" else gen.max_out_degree_vertex(pairs[:imported], V)
+    g = gpu_graph(algo, V, pairs[:imported], hint=len(pairs), inc_mode=True)
+    g.set_option("cluster_edges", cluster_edges)
+    g.set_option("fused_max", 0)   # every batch through the grid-wide kernels and the level loop
+    og = oracle_graph(algo, V, pairs[:imported], inc_mode=True)
+    og.build_tree(root)
+    g.build_tree(algo, root)
+    np.testing.assert_array_equal(g.values(), og.labels()[0])
+    assert (g.level_device_times() >= 0).all()
+    batch, nb = 2000, 5
+    ref = og.run_batch(pairs, imported, batch, nb, root)
+    e = edges_of(algo, pairs)
+    for k in range(nb):
+        lo = imported + k * batch
+        g.apply_add(algo, e[lo:lo + batch], directed)
+        g.apply_del(algo, e[lo - imported:lo - imported + batch], directed)
+        assert g.checksum() == int(ref[k]), f"batch {k}"
+    val, par, pw = g.labels()
+    assert og.validate(val, par, pw, root) == 0
+    g.close()
