@@ -373,7 +373,10 @@ typedef struct {
 int rg_server_create(uint64_t hbm_budget_bytes, double target_epoch_ms, uint64_t max_epoch, int per_update,
                      rg_server **out);
 /* Admit a graph (labels already built with rg_build_tree for `algo`).
- * RG_ENOMEM_HBM when its device bytes would exceed the budget. */
+ * RG_ENOMEM_HBM when its device bytes would exceed the budget.  While
+ * attached the graph runs no cluster levels (RG_OPT_CLUSTER_EDGES reads 0;
+ * detach gives the value back): with other instances' epochs on the GPU a
+ * level that needs a GPC of free SMs at once would wait for them. */
 int rg_server_attach(rg_server *s, rg_graph *g, int algo, int directed, uint32_t *instance);
 int rg_server_detach(rg_server *s, uint32_t instance);
 /* Record the label history (rg_history_record of the modified vertices) after

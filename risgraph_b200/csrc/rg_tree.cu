@@ -135,17 +135,26 @@ __global__ void __launch_bounds__(TPB) k_push(DevGraph g, const uint32_t *fin, c
     uint64_t i = base + lane;
     uint32_t u = 0, len = 0;
     uint64_t off = 0, su = 0;
+    uint32_t hub_c = 0;            // tasks of this lane's hub list
+    unsigned long long hub_k = 0;  // where they go in the task queue
     if (lane < vpw && i < n) {
       u = fin[i];
       len = seg_len(g.out, u);
       off = g.out.off[u];
       su = ld_v32(g.val32, u);
       if (len > HUB) {
-        uint32_t nch = (len + CHUNK - 1) / CHUNK;
-        unsigned long long k = atomicAdd(hub_n, (unsigned long long)nch);
-        for (uint32_t c = 0; c < nch; c++) hubq[k + c] = (uint64_t)u | ((uint64_t)c << 32);
+        hub_c = (len + CHUNK - 1) / CHUNK;
+        hub_k = atomicAdd(hub_n, (unsigned long long)hub_c);
         len = 0;
       }
+    }
+    // the whole warp writes each hub's task list (a hub of 100K slots has 1,563
+    // tasks: one lane writing them alone took longer than the rest of the level)
+    for (unsigned hm = __ballot_sync(FULL, hub_c != 0); hm; hm &= hm - 1) {
+      const int src = __ffs(hm) - 1;
+      const uint32_t hu = __shfl_sync(FULL, u, src), hc = __shfl_sync(FULL, hub_c, src);
+      const unsigned long long hk = __shfl_sync(FULL, hub_k, src);
+      for (uint32_t c = lane; c < hc; c += 32) hubq[hk + c] = (uint64_t)hu | ((uint64_t)c << 32);
     }
     uint32_t incl = len;
 #pragma unroll

@@ -148,3 +148,20 @@ def test_open_loop_poisson_load():
         srv.detach(k)
     assert r["completed"] == 1500 and r["failed"] == 0
     np.testing.assert_array_equal(inst["g"].values(), expected_values(inst, r["adds"], r["dels"]))
+
+
+def test_attached_graphs_run_no_cluster_levels():
+    """A served graph runs without cluster levels (other instances' epochs keep
+    SMs busy, and a cluster level waits for a GPC of free SMs); detach gives
+    the graph its setting back, and served values still match."""
+    inst = make_instance("sssp", 12, 4)
+    g = inst["g"]
+    g.set_option("cluster_edges", 1 << 20)
+    with rg.Server(max_epoch=4096) as srv:
+        k = srv.attach(g)
+        assert g.get_option("cluster_edges") == 0
+        r, = srv.run_load([load_of(inst, k, 16, 2000, 3)])
+        srv.detach(k)
+    assert g.get_option("cluster_edges") == 1 << 20
+    assert r["completed"] == 2000 and r["failed"] == 0
+    np.testing.assert_array_equal(g.values(), expected_values(inst, r["adds"], r["dels"]))
