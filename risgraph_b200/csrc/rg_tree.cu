@@ -1335,7 +1335,10 @@ struct LevelCfg {
 // Picks the level mode from the frontier size (the reference's push/pull rule
 // at core/graph.hpp:334 and its vertex/edge-centric rule at :595-612 play the
 // same role); inside a graph it also selects the SWITCH case to run.
-constexpr int LVB_TPB = 1024;  // threads of k_level_begin (they sum small frontiers' degrees)
+// Threads of k_level_begin (they sum small frontiers' degrees).  256, not
+// 1024: the kernel starts every level, and in served mode the epochs of other
+// instances occupy the SMs, where a 1024-thread CTA waits longer for room.
+constexpr int LVB_TPB = 256;
 // A frontier that both a tiny level and a cluster level could take goes to the
 // cluster when it has more out-slots than this: one CTA walks them
 // 1024 at a time, the cluster 16,384 at a time.
@@ -1349,16 +1352,16 @@ __global__ void __launch_bounds__(LVB_TPB) k_level_begin(DevGraph g, const uint3
   const uint64_t n0 = *fin_n;
   unsigned long long d = 0;
   if ((cfg.tiny_edges && n0 && n0 <= TINY_N) || (cfg.cl_edges && n0 && n0 <= cfg.cl_v)) {
-    // four frontier entries per thread in flight (a frontier of up to 16K vertices)
-    for (uint64_t i0 = threadIdx.x; i0 < n0; i0 += 4 * LVB_TPB) {
-      uint32_t u[4];
+    // eight frontier entries per thread in flight (a frontier of up to 16K vertices)
+    for (uint64_t i0 = threadIdx.x; i0 < n0; i0 += 8 * LVB_TPB) {
+      uint32_t u[8];
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < 8; k++) {
         const uint64_t i = i0 + (uint64_t)k * LVB_TPB;
         u[k] = i < n0 ? fin[i] : NONE;
       }
 #pragma unroll
-      for (int k = 0; k < 4; k++) d += u[k] != NONE ? seg_len(g.out, u[k]) : 0u;
+      for (int k = 0; k < 8; k++) d += u[k] != NONE ? seg_len(g.out, u[k]) : 0u;
     }
   }
   // a tree reduction: 1024 threads adding into one shared word contend for it
