@@ -55,7 +55,9 @@ THROTTLE_BITS = {
     0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
     0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
 }
-ALL_LEGS = ["builds", "bfs_inc", "batches", "served", "served_mix", "wcc_del"]
+# the six-instance mix runs right after the builds: its latency is the most sensitive to what
+# earlier legs leave behind in the process (it measured alike alone and in this position)
+ALL_LEGS = ["builds", "served_mix", "bfs_inc", "batches", "served", "wcc_del"]
 
 
 def parse():
@@ -832,7 +834,9 @@ def main():
                "bfs_inc": lambda: leg_bfs_inc(args),
                "batches": lambda: leg_batches(args), "served": lambda: leg_served(args),
                "served_mix": lambda: leg_served_mix(args), "wcc_del": lambda: leg_wcc_del(args)}
+        import gc
         for name in want:
+            gc.collect()   # what earlier legs left is freed now, not inside a timed load
             t = time.time()
             print(f"[bench] leg {name} ...", file=sys.stderr, flush=True)
             try:
