@@ -4,8 +4,6 @@ import ctypes
 import glob
 import os
 
-import pytest
-
 import risgraph_b200 as rg
 
 INCLUDE = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include")
